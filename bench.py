@@ -1,0 +1,313 @@
+"""Benchmark of the B200 BPC-PaCo codec.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--config cfg2]
+
+One step = encode + decode of one synthetic image of the named configuration
+(default cfg2: 4096x4096, 5-level CDF 5/3 DWT, 64x64 codeblocks, 3 passes).
+`value` is coefficients coded per second counting both directions,
+2 * X * Y / (t_encode + t_decode), with each kernel timed by CUDA events on its
+launching stream and the L2 flushed (a 256 MiB write) before every kernel;
+`e2e` is the same metric through the C ABI's host-buffer call (bpc_code_host:
+pinned host -> device copy, kernel, device -> host copy, status read).
+Under torchrun (N > 1) every rank codes its own image (weak scaling, no
+collective on the data path) and the time is the max over ranks.
+
+--impl reference times the CPU restatement of the reference coder (the
+reference has no CPU implementation of its own) on all host cores, on a
+bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "cuda_bpc-paco_b200")
+sys.path.insert(0, PKG)
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+LUT_DIR = os.path.join(ROOT, "tests", "golden", "luts")
+
+CONFIGS = {
+    # name: side, levels, passes, cb, amp, nrect
+    "cfg1": dict(side=2048, levels=5, passes=2, cb=64, amp=20.0, nrect=30),
+    "cfg2": dict(side=4096, levels=5, passes=3, cb=64, amp=40.0, nrect=60),
+    "cfg5": dict(side=16384, levels=5, passes=3, cb=64, amp=80.0, nrect=400),
+}
+METRIC = "encode/decode Gcoeff/s (bit-exact)"
+
+
+def workload_name(c):
+    return (f"{c['side']}x{c['side']} synthetic image, {c['levels']}-level CDF 5/3 DWT, "
+            f"{c['cb']}x{c['cb']} codeblocks, {c['passes']}-pass encode+decode")
+
+
+def load_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled during the timed region."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.samples = []
+        self.proc = None
+        self.thread = None
+
+    def __enter__(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 7:
+                self.samples.append(parts)
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for s in self.samples for k in range(4) if s[3 + k].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def dist_info():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def cpu_baseline(img, lut_np, c, budget_s=12.0):
+    """Oracle (CPU restatement) encode + decode on all host cores over a
+    bounded prefix of the codeblocks."""
+    import oracle
+    threads = os.cpu_count() or 1
+    ncb = (img.shape[0] // c["cb"]) * (img.shape[1] // c["cb"])
+    # calibrate on a small prefix, then size the sample to ~budget_s
+    n = min(ncb, max(threads * 4, 64))
+    t0 = time.perf_counter()
+    s = oracle.encode(img, lut_np, c["passes"], c["levels"], c["cb"], threads, cb_range=(0, n))
+    oracle.decode(s, img.shape, lut_np, c["passes"], c["levels"], c["cb"], threads, cb_range=(0, n))
+    dt = time.perf_counter() - t0
+    n2 = int(min(ncb, max(n, n * budget_s / max(dt, 1e-3))))
+    t0 = time.perf_counter()
+    s = oracle.encode(img, lut_np, c["passes"], c["levels"], c["cb"], threads, cb_range=(0, n2))
+    oracle.decode(s, img.shape, lut_np, c["passes"], c["levels"], c["cb"], threads, cb_range=(0, n2))
+    dt = time.perf_counter() - t0
+    coefs = n2 * c["cb"] * c["cb"]
+    return {"value": 2 * coefs / dt / 1e9, "unit": "Gcoeff/s", "cores": threads, "kind": "port",
+            "sample": f"first {n2} of {ncb} codeblocks of the same image, encode+decode, {dt:.1f} s"}
+
+
+def make_input(c, seed):
+    import bpc_synth
+    return bpc_synth.synthetic_coefficients(c["side"], c["levels"], seed, amp=c["amp"], nrect=c["nrect"])
+
+
+def run_reference(args, c):
+    rank, world, _ = dist_info()
+    if rank != 0:
+        return
+    import oracle
+    img = make_input(c, 1)
+    lut_np = oracle.load_luts(os.path.join(LUT_DIR, f"{c['passes']}_coding_pass"), c["passes"], c["levels"])
+    threads = os.cpu_count() or 1
+    ncb = (img.shape[0] // c["cb"]) * (img.shape[1] // c["cb"])
+    n = min(ncb, max(threads * 8, 128))
+    times = []
+    for k in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        s = oracle.encode(img, lut_np, c["passes"], c["levels"], c["cb"], threads, cb_range=(0, n))
+        oracle.decode(s, img.shape, lut_np, c["passes"], c["levels"], c["cb"], threads, cb_range=(0, n))
+        if k >= args.warmup:
+            times.append(time.perf_counter() - t0)
+    coefs = n * c["cb"] * c["cb"]
+    v = 2 * coefs * len(times) / sum(times) / 1e9
+    sample = f"first {n} of {ncb} codeblocks per step, encode+decode, CPU restatement"
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "Gcoeff/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(times) / len(times),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+        "data": "synthetic", "config": {"workload": workload_name(c), "l2": "n/a (CPU)"},
+        "cpu_baseline": {"value": v, "unit": "Gcoeff/s", "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": v, "unit": "Gcoeff/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
+
+
+def run_ours(args, c):
+    import torch
+    import bpc_paco as bpc
+
+    rank, world, local = dist_info()
+    dist = world > 1
+    if dist:
+        import torch.distributed as tdist
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        tdist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    dev = torch.device("cuda", local if dist else 0)
+    torch.cuda.set_device(dev)
+    img = make_input(c, 1 + rank)
+    X = Y = c["side"]
+    N = X * Y
+    passes, levels, cb = c["passes"], c["levels"], c["cb"]
+    lut = bpc.DeviceLut(os.path.join(LUT_DIR, f"{passes}_coding_pass"), passes, levels)
+    stream = torch.cuda.current_stream()
+    d_img = torch.from_numpy(img).to(dev)
+    d_stream = torch.empty(N, dtype=torch.int32, device=dev)
+    d_dec = torch.empty_like(d_img)
+    d_status = torch.zeros(1, dtype=torch.int32, device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+
+    def step(times=None):
+        flush.fill_(1)
+        e0, e1, e2, e3 = (torch.cuda.Event(enable_timing=True) for _ in range(4))
+        e0.record(stream)
+        bpc.encode_device(d_img, d_stream, lut, cb, d_status)
+        e1.record(stream)
+        flush.fill_(2)
+        e2.record(stream)
+        bpc.decode_device(d_stream, d_dec, lut, cb, d_status)
+        e3.record(stream)
+        if times is not None:
+            times.append((e0, e1, e2, e3))
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+    # bit-exactness of this run's output (decode must return the input)
+    assert torch.equal(d_dec, d_img), "decode did not return the input"
+    assert d_status.item() == 0, f"status {d_status.item()}"
+
+    times = []
+    if dist:
+        tdist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local if dist else 0) as clk:
+        w0 = time.perf_counter()
+        for _ in range(args.steps):
+            step(times)
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - w0
+    if dist:
+        tdist.barrier()
+    te = sum(a.elapsed_time(b) for a, b, _, _ in times) / 1e3
+    td = sum(c2.elapsed_time(d) for _, _, c2, d in times) / 1e3
+    t_step = (te + td) / args.steps
+    if dist:
+        t = torch.tensor([t_step], dtype=torch.float64, device=dev)
+        tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
+        t_step = float(t.item())
+    value = 2 * N * world / t_step / 1e9
+
+    # e2e through the C ABI with pinned host buffers (copies inside the timed region)
+    h = torch.empty(N, dtype=torch.int32, pin_memory=True)
+    hn = h.numpy()
+    ref_stream = d_stream.cpu().numpy()
+    e2e_t = []
+    for k in range(max(args.warmup, 3) + args.steps):
+        hn[:] = img.reshape(-1)
+        t0 = time.perf_counter()
+        st1 = bpc.lib().bpc_code_host(bpc.CODE, hn.ctypes.data, X, Y, bpc.ctypes.c_void_p(lut.ptr), lut.n,
+                                      passes, levels, cb)
+        t1 = time.perf_counter()
+        if k == 0:
+            assert np.array_equal(hn, ref_stream), "host-path stream differs from device-path stream"
+        t2 = time.perf_counter()
+        st2 = bpc.lib().bpc_code_host(bpc.DECODE, hn.ctypes.data, X, Y, bpc.ctypes.c_void_p(lut.ptr), lut.n,
+                                      passes, levels, cb)
+        t3 = time.perf_counter()
+        assert st1 == 0 and st2 == 0
+        if k >= max(args.warmup, 3):
+            e2e_t.append((t1 - t0) + (t3 - t2))
+    assert np.array_equal(hn.reshape(Y, X), img), "host-path decode differs"
+    e2e_step = float(np.mean(e2e_t))
+    if dist:
+        t = torch.tensor([e2e_step], dtype=torch.float64, device=dev)
+        tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
+        e2e_step = float(t.item())
+    e2e = 2 * N * world / e2e_step / 1e9
+
+    peak, peak_kind = load_peaks()
+    alg_bytes = 8.0 * N  # per launch: 4 B/coef in + 4 B/coef out (slot stream), encode and decode alike
+    te1, td1 = te / args.steps, td / args.steps
+    dom_t = max(te1, td1)
+    achieved = alg_bytes / dom_t / 1e9
+    line = {
+        "metric": METRIC, "value": value, "unit": "Gcoeff/s", "n_gpus": world, "steps": args.steps,
+        "warmup": max(args.warmup, 3), "ms_per_step": 1e3 * t_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded generator + 5/3 DWT)",
+        "config": {"workload": workload_name(c), "name": args.config, "coefficients_per_gpu": N,
+                   "l2": "flushed (256 MiB write) before every kernel", "parallelism": f"replicas x{world}"},
+        "encode_gcoeffs": N / te1 / 1e9, "decode_gcoeffs": N / td1 / 1e9,
+        "e2e": {"value": e2e, "unit": "Gcoeff/s", "h2d_bytes_per_step": 2 * 4 * N, "d2h_bytes_per_step": 2 * 4 * N + 8},
+        "gpu_launches": 2 * args.steps,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": None, "peak_source": peak_kind,
+                     "kernel": "k_bpc decoder" if td1 >= te1 else "k_bpc encoder",
+                     "note": "8 B/coefficient algorithmic; the coder is bound by SM integer issue, not HBM"},
+        "clocks": clk.summary(), "wall_s_timed": wall,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        lut_np = bpc.load_luts_host(os.path.join(LUT_DIR, f"{passes}_coding_pass"), passes, levels)
+        line["cpu_baseline"] = cpu_baseline(img, lut_np, c)
+    lut.close()
+    if dist:
+        tdist.barrier()
+        tdist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="cfg2", choices=sorted(CONFIGS))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    c = CONFIGS[args.config]
+    if args.impl == "reference":
+        run_reference(args, c)
+    else:
+        run_ours(args, c)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,180 @@
+"""Python binding of the codec's C ABI (include/bpc_paco.h).
+
+It mirrors the reference's host interface (source/main_example.cu:8 CUDA_BPC,
+:219 load_LUTs) and exposes the device-pointer entry points for callers that
+keep data on the GPU (torch tensors are accepted there; torch is only used for
+device memory and streams).  The library is the in-tree libbpc_paco.so; if it
+is missing this module raises instead of falling back to anything else.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libbpc_paco.so")
+
+CODE, DECODE = 0, 1
+OK = 0
+ERR_ARG, ERR_CUDA, ERR_FILE, ERR_PARSE, ERR_NOMEM = -1, -2, -3, -4, -5
+ST_SLOT_OVERFLOW, ST_BAD_STREAM, ST_INPUT_RANGE, ST_LUT_RANGE = 1, 2, 4, 8
+
+EXPORTS = ("CUDA_BPC", "load_LUTs", "bpc_set_mode", "bpc_get_mode", "bpc_last_status", "bpc_status_string",
+           "bpc_load_luts_host", "bpc_load_luts", "bpc_lut_free", "bpc_code_host", "bpc_encode_device",
+           "bpc_decode_device", "bpc_lut_entries", "bpc_version")
+
+_lib = None
+
+
+class BpcError(RuntimeError):
+    pass
+
+
+def lib() -> ctypes.CDLL:
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise BpcError(f"{LIB_PATH} is missing: build it with `python cuda_bpc-paco_b200/build.py`")
+        L = ctypes.CDLL(LIB_PATH)
+        ip = ctypes.POINTER(ctypes.c_int)
+        vp = ctypes.c_void_p
+        L.CUDA_BPC.argtypes = [ctypes.c_int, vp, ctypes.c_int, ctypes.c_int, vp]
+        L.CUDA_BPC.restype = None
+        L.load_LUTs.argtypes = [ctypes.POINTER(vp), ctypes.c_char_p]
+        L.load_LUTs.restype = None
+        L.bpc_set_mode.argtypes = [ctypes.c_int] * 3
+        L.bpc_get_mode.argtypes = [ip, ip, ip]
+        L.bpc_last_status.argtypes = []
+        L.bpc_status_string.argtypes = [ctypes.c_int]
+        L.bpc_status_string.restype = ctypes.c_char_p
+        L.bpc_load_luts_host.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, vp, ctypes.c_int, ip]
+        L.bpc_load_luts.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.POINTER(vp), ip]
+        L.bpc_lut_free.argtypes = [vp]
+        L.bpc_code_host.argtypes = [ctypes.c_int, vp, ctypes.c_int, ctypes.c_int, vp, ctypes.c_int, ctypes.c_int,
+                                    ctypes.c_int, ctypes.c_int]
+        dev = [vp, vp, ctypes.c_int, ctypes.c_int, vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp, vp,
+               ctypes.c_int, vp]
+        L.bpc_encode_device.argtypes = dev
+        L.bpc_decode_device.argtypes = dev
+        L.bpc_lut_entries.argtypes = [ctypes.c_int] * 3
+        for f in ("bpc_set_mode", "bpc_get_mode", "bpc_last_status", "bpc_load_luts_host", "bpc_load_luts",
+                  "bpc_lut_free", "bpc_code_host", "bpc_encode_device", "bpc_decode_device", "bpc_lut_entries",
+                  "bpc_version"):
+            getattr(L, f).restype = ctypes.c_int
+        _lib = L
+    return _lib
+
+
+def status_string(st: int) -> str:
+    return lib().bpc_status_string(st).decode()
+
+
+def _check(rc: int, what: str) -> int:
+    if rc < 0:
+        raise BpcError(f"{what}: {status_string(rc)} ({rc})")
+    return rc
+
+
+def _folder(folder: str) -> bytes:
+    return (folder if folder.endswith("/") else folder + "/").encode()
+
+
+# ----------------------------------------------------------------- drop-in
+def set_mode(passes: int, levels: int = 5, cb: int = 64) -> None:
+    _check(lib().bpc_set_mode(passes, levels, cb), "bpc_set_mode")
+
+
+def get_mode():
+    a, b, c = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+    lib().bpc_get_mode(ctypes.byref(a), ctypes.byref(b), ctypes.byref(c))
+    return a.value, b.value, c.value
+
+
+def load_LUTs(folder: str) -> int:
+    """Reference load_LUTs: returns the device pointer (int), 0 on error."""
+    p = ctypes.c_void_p()
+    lib().load_LUTs(ctypes.byref(p), _folder(folder))
+    return p.value or 0
+
+
+def CUDA_BPC(direction: int, hdata: np.ndarray, X: int, Y: int, lut_ptr: int) -> int:
+    """Reference CUDA_BPC: codes `hdata` (int32, X*Y, C-contiguous) in place;
+    frees the LUT.  Returns bpc_last_status()."""
+    assert hdata.dtype == np.int32 and hdata.flags["C_CONTIGUOUS"] and hdata.size == X * Y
+    lib().CUDA_BPC(direction, hdata.ctypes.data, X, Y, ctypes.c_void_p(lut_ptr))
+    return lib().bpc_last_status()
+
+
+# -------------------------------------------------------- explicit variants
+def load_luts_host(folder: str, passes: int, levels: int = 5) -> np.ndarray:
+    n = ctypes.c_int(0)
+    _check(lib().bpc_load_luts_host(_folder(folder), passes, levels, None, 0, ctypes.byref(n)), "load_luts_host")
+    out = np.zeros(n.value, np.int32)
+    _check(lib().bpc_load_luts_host(_folder(folder), passes, levels, out.ctypes.data, out.size, ctypes.byref(n)),
+           "load_luts_host")
+    return out
+
+
+class DeviceLut:
+    """A LUT resident on the device (bpc_load_luts / bpc_lut_free)."""
+
+    def __init__(self, folder: str, passes: int, levels: int = 5):
+        p, n = ctypes.c_void_p(), ctypes.c_int(0)
+        _check(lib().bpc_load_luts(_folder(folder), passes, levels, ctypes.byref(p), ctypes.byref(n)), "load_luts")
+        self.ptr, self.n, self.passes, self.levels = p.value, n.value, passes, levels
+
+    def close(self) -> None:
+        if self.ptr:
+            lib().bpc_lut_free(ctypes.c_void_p(self.ptr))
+            self.ptr = 0
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def encode_host(img: np.ndarray, lut: DeviceLut, cb: int = 64) -> tuple[np.ndarray, int]:
+    buf = np.ascontiguousarray(img, dtype=np.int32).copy()
+    Y, X = buf.shape
+    st = _check(lib().bpc_code_host(CODE, buf.ctypes.data, X, Y, ctypes.c_void_p(lut.ptr), lut.n, lut.passes,
+                                    lut.levels, cb), "bpc_code_host")
+    return buf.reshape(-1), st
+
+
+def decode_host(stream: np.ndarray, shape, lut: DeviceLut, cb: int = 64) -> tuple[np.ndarray, int]:
+    Y, X = shape
+    buf = np.ascontiguousarray(stream, dtype=np.int32).reshape(-1).copy()
+    assert buf.size == X * Y
+    st = _check(lib().bpc_code_host(DECODE, buf.ctypes.data, X, Y, ctypes.c_void_p(lut.ptr), lut.n, lut.passes,
+                                    lut.levels, cb), "bpc_code_host")
+    return buf.reshape(Y, X), st
+
+
+def _ptr(t) -> int:
+    return 0 if t is None else int(t.data_ptr())
+
+
+def encode_device(coeffs, stream_out, lut: DeviceLut, cb: int = 64, status=None, counts=None, grid: int = 0,
+                  cuda_stream: int | None = None) -> None:
+    """Device-to-device encode of torch int32 tensors (Y x X coeffs -> X*Y
+    stream), enqueued on `cuda_stream` (default: torch's current stream)."""
+    import torch
+    Y, X = coeffs.shape
+    s = torch.cuda.current_stream().cuda_stream if cuda_stream is None else cuda_stream
+    _check(lib().bpc_encode_device(_ptr(coeffs), _ptr(stream_out), X, Y, ctypes.c_void_p(lut.ptr), lut.n, lut.passes,
+                                   lut.levels, cb, ctypes.c_void_p(_ptr(status)), ctypes.c_void_p(_ptr(counts)), grid,
+                                   ctypes.c_void_p(s)), "bpc_encode_device")
+
+
+def decode_device(stream_in, coeffs_out, lut: DeviceLut, cb: int = 64, status=None, counts=None, grid: int = 0,
+                  cuda_stream: int | None = None) -> None:
+    import torch
+    Y, X = coeffs_out.shape
+    s = torch.cuda.current_stream().cuda_stream if cuda_stream is None else cuda_stream
+    _check(lib().bpc_decode_device(_ptr(stream_in), _ptr(coeffs_out), X, Y, ctypes.c_void_p(lut.ptr), lut.n,
+                                   lut.passes, lut.levels, cb, ctypes.c_void_p(_ptr(status)),
+                                   ctypes.c_void_p(_ptr(counts)), grid, ctypes.c_void_p(s)), "bpc_decode_device")

@@ -1,0 +1,100 @@
+// bpc_kernels.cu -- sm_100a kernels of the BPC-PaCo coder and their launcher.
+//
+// One warp codes one 64x64 codeblock (or two 32x32 codeblocks); a CTA of
+// kWarps warps stages the LUT once into shared memory as bytes and then walks
+// codeblocks grid-stride, so the same kernel serves the plain one-image launch
+// (grid = ceil(ncb / kWarps)) and a persistent launch (grid = k * 148).
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "bpc_core.cuh"
+#include "bpc_kernels.h"
+
+namespace bpc {
+
+struct GpuWarp {
+    __device__ __forceinline__ int lane() const { return (int)(threadIdx.x & 31u); }
+    __device__ __forceinline__ uint32_t ballot(bool p) { return __ballot_sync(0xffffffffu, p); }
+    __device__ __forceinline__ bool any(bool p) { return __any_sync(0xffffffffu, p) != 0; }
+    __device__ __forceinline__ uint32_t shfl_xor(uint32_t v, int o) { return __shfl_xor_sync(0xffffffffu, v, o); }
+    __device__ __forceinline__ uint32_t shfl_up(uint32_t v, int d) { return __shfl_up_sync(0xffffffffu, v, d); }
+    __device__ __forceinline__ uint32_t shfl_down(uint32_t v, int d) { return __shfl_down_sync(0xffffffffu, v, d); }
+    __device__ __forceinline__ void sync() { __syncwarp(); }
+    __device__ __forceinline__ void syncmask(uint32_t m) { __syncwarp(m); }
+    __device__ __forceinline__ void load2(const int32_t *p, int32_t &a, int32_t &b) {
+        const int2 v = __ldg(reinterpret_cast<const int2 *>(p));
+        a = v.x;
+        b = v.y;
+    }
+    __device__ __forceinline__ void store2(int32_t *p, int32_t a, int32_t b) {
+        *reinterpret_cast<int2 *>(p) = make_int2(a, b);
+    }
+    __device__ __forceinline__ void load4(const int32_t *p, uint32_t &a, uint32_t &b, uint32_t &c, uint32_t &d) {
+        const int4 v = __ldg(reinterpret_cast<const int4 *>(p));
+        a = (uint32_t)v.x;
+        b = (uint32_t)v.y;
+        c = (uint32_t)v.z;
+        d = (uint32_t)v.w;
+    }
+    __device__ __forceinline__ void atomic_or(int *p, int v) { atomicOr(p, v); }
+};
+
+template <int PASSES, int CBS, bool ENC>
+__global__ void __launch_bounds__(kWarps * 32) k_bpc(Params p) {
+    using G = Geo<CBS>;
+    extern __shared__ __align__(16) unsigned char smem[];
+    uint8_t *tab = smem;
+    int bad = 0;
+    for (int k = (int)threadIdx.x; k < p.tab_n; k += (int)blockDim.x) {
+        int v = k < p.lut_n ? __ldg(p.lut + k) : 0;
+        if (v < 0 || v > 255) {
+            bad = 1;
+            v = 0;
+        }
+        tab[k] = (uint8_t)v;
+    }
+    if (bad && p.status) atomicOr(p.status, ST_LUT_RANGE);
+    __syncthreads();
+    const int warp = (int)(threadIdx.x >> 5);
+    uint32_t *words = reinterpret_cast<uint32_t *>(smem + p.tab_n);
+    uint32_t *mag = words + warp * G::MAG_WORDS;
+    uint32_t *ring = words + kWarps * G::MAG_WORDS + warp * G::RING_WORDS;
+    GpuWarp w;
+    const int stride = (int)gridDim.x * kWarps * G::NG;
+    for (int base = ((int)blockIdx.x * kWarps + warp) * G::NG; base < p.ncb; base += stride) {
+        Coder<PASSES, CBS, ENC, GpuWarp> cd(w, p, mag, ring, tab);
+        cd.run(base);
+    }
+}
+
+template <int PASSES, int CBS, bool ENC>
+static size_t smem_bytes(const Params &p) {
+    using G = Geo<CBS>;
+    return (size_t)p.tab_n + (size_t)kWarps * 4u * (size_t)(G::MAG_WORDS + (ENC ? 0 : G::RING_WORDS));
+}
+
+template <int PASSES, int CBS, bool ENC>
+static cudaError_t launch_t(const Params &p, int grid, cudaStream_t st) {
+    using G = Geo<CBS>;
+    const size_t sm = smem_bytes<PASSES, CBS, ENC>(p);
+    cudaError_t e = cudaFuncSetAttribute(k_bpc<PASSES, CBS, ENC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return e;
+    const int warps_needed = (p.ncb + G::NG - 1) / G::NG;
+    const int full = (warps_needed + kWarps - 1) / kWarps;
+    if (grid <= 0 || grid > full) grid = full;
+    if (grid < 1) grid = 1;
+    k_bpc<PASSES, CBS, ENC><<<grid, kWarps * 32, sm, st>>>(p);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_code(bool enc, int passes, int cbs, const Params &p, int grid, cudaStream_t st) {
+    if (p.ncb <= 0) return cudaSuccess;
+    if (enc) {
+        if (passes == 2) return cbs == 64 ? launch_t<2, 64, true>(p, grid, st) : launch_t<2, 32, true>(p, grid, st);
+        return cbs == 64 ? launch_t<3, 64, true>(p, grid, st) : launch_t<3, 32, true>(p, grid, st);
+    }
+    if (passes == 2) return cbs == 64 ? launch_t<2, 64, false>(p, grid, st) : launch_t<2, 32, false>(p, grid, st);
+    return cbs == 64 ? launch_t<3, 64, false>(p, grid, st) : launch_t<3, 32, false>(p, grid, st);
+}
+
+}  // namespace bpc

@@ -1,0 +1,116 @@
+/*
+ * bpc_paco.h -- C ABI of the B200 (sm_100a) BPC-PaCo codec.
+ *
+ * Drop-in for the host call surface of PabloEnfedaque/CUDA_BPC-PaCo: the same
+ * entry points source/main_example.cu calls (CUDA_BPC, load_LUTs), the same
+ * buffers (raster int32 DWT coefficients; an X*Y-int stream of codeblock-major
+ * slots: slot[0] = MSB, slot[1..n] = 16-bit codewords in reservation order,
+ * the rest -1), the same LUT text format and a bit-identical bitstream.
+ *
+ * Plain C types only (pointers, ints); `stream` arguments are cudaStream_t
+ * passed as void*.  All functions are thread-compatible, not thread-safe:
+ * serialise calls that share a LUT or the drop-in mode.
+ */
+#ifndef BPC_PACO_H
+#define BPC_PACO_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Direction: the reference's enum BPC {CODE, DECODE} (source/common.h:8-11). */
+enum { BPC_CODE = 0, BPC_DECODE = 1 };
+
+/* Return values.  0 = success.  Negative = the call failed and did nothing
+ * useful.  Positive = the call ran; the value is the OR of per-codeblock
+ * conditions (the outputs of the affected codeblocks are defined but differ
+ * from what the reference would produce, whose behaviour there is undefined):
+ *   SLOT_OVERFLOW  more codewords than the slot holds (4095 for 64x64); the
+ *                  excess is dropped instead of spilling into the next slot;
+ *   BAD_STREAM     a slot whose MSB word is outside 0..32 (decoded as zeros);
+ *   INPUT_RANGE    a coefficient with |x| >= 2^28 (flag bits would collide);
+ *   LUT_RANGE      a LUT entry outside 0..255 (read as 0). */
+#define BPC_OK 0
+#define BPC_ERR_ARG (-1)
+#define BPC_ERR_CUDA (-2)
+#define BPC_ERR_FILE (-3)
+#define BPC_ERR_PARSE (-4)
+#define BPC_ERR_NOMEM (-5)
+#define BPC_ST_SLOT_OVERFLOW 1
+#define BPC_ST_BAD_STREAM 2
+#define BPC_ST_INPUT_RANGE 4
+#define BPC_ST_LUT_RANGE 8
+
+/* ---------------------------------------------------------------------------
+ * Drop-in entry points
+ * ------------------------------------------------------------------------- */
+
+/* Replaces CUDA_BPC, source/BPC_PaCo.cu:1305-1325 (declared at
+ * source/main_example.cu:8).  Direction BPC_CODE: HData holds HDSize_X x
+ * HDSize_Y raster coefficients and is overwritten with the slot stream;
+ * BPC_DECODE: the reverse.  LUT is a device pointer from load_LUTs and, as in
+ * the reference (:1300), this call frees it.  Synchronous.  The coding mode
+ * (passes, DWT levels, codeblock size) is the one set with bpc_set_mode,
+ * replacing the reference's -DCPASS_3 / -DDWT_LEVELS / -DCBLOCK_LENGTH.
+ * Errors are reported on stderr and kept for bpc_last_status(); unlike the
+ * reference (common.cu:3-9) it never calls exit(). */
+void CUDA_BPC(int Direction, int *HData, int HDSize_X, int HDSize_Y, int *LUT);
+
+/* Replaces load_LUTs, source/main_example.cu:219-448: parses ref.txt,
+ * sig.txt, sign.txt (+ cp_sig.txt, cp_sign.txt in 3-pass mode) from `folder`
+ * (a prefix, so it normally ends in '/') with the reference's rules and
+ * uploads the array to a new device buffer stored in *LUT (NULL on error). */
+void load_LUTs(int **LUT, const char *folder);
+
+/* Mode for CUDA_BPC / load_LUTs: passes 2 or 3 (CPASS_3 = 0 / 1), DWT levels
+ * >= 1, codeblock size 64 (the reference) or 32.  Default 2, 5, 64. */
+int bpc_set_mode(int passes, int dwt_levels, int cb_size);
+int bpc_get_mode(int *passes, int *dwt_levels, int *cb_size);
+
+/* Status of the last drop-in call (CUDA_BPC / load_LUTs) on this process. */
+int bpc_last_status(void);
+const char *bpc_status_string(int status);
+
+/* ---------------------------------------------------------------------------
+ * Status-returning variants
+ * ------------------------------------------------------------------------- */
+
+/* load_LUTs into host memory.  With out == NULL only *n_entries is set. */
+int bpc_load_luts_host(const char *folder, int passes, int levels, int *out, int capacity, int *n_entries);
+
+/* load_LUTs into a new device buffer (free with bpc_lut_free). */
+int bpc_load_luts(const char *folder, int passes, int levels, int **d_lut, int *n_entries);
+int bpc_lut_free(int *d_lut);
+
+/* CUDA_BPC with explicit mode and LUT length, returning the status; does not
+ * free the LUT.  hdata is host memory (pinned memory is fastest). */
+int bpc_code_host(int direction, int *hdata, int X, int Y, const int *d_lut, int lut_n, int passes, int levels,
+                  int cb_size);
+
+/* ---------------------------------------------------------------------------
+ * Device-pointer entry points: stream-ordered, no allocation, no host sync.
+ * ------------------------------------------------------------------------- */
+
+/* Encode X x Y raster coefficients (device) into the slot stream (device,
+ * X*Y ints).  X and Y must be multiples of cb_size.  d_status (device int,
+ * may be NULL) receives the OR of BPC_ST_* bits (the caller zeroes it);
+ * d_counts (device, one int per codeblock, may be NULL) receives the number
+ * of codewords of each codeblock.  grid = 0 launches one CTA per 4
+ * codeblocks; grid > 0 launches that many persistent CTAs. */
+int bpc_encode_device(const int *d_coeffs, int *d_stream, int X, int Y, const int *d_lut, int lut_n, int passes,
+                      int levels, int cb_size, int *d_status, int *d_counts, int grid, void *stream);
+
+/* Decode the slot stream (device) into raster coefficients (device). */
+int bpc_decode_device(const int *d_stream, int *d_coeffs, int X, int Y, const int *d_lut, int lut_n, int passes,
+                      int levels, int cb_size, int *d_status, int *d_counts, int grid, void *stream);
+
+/* Number of ints of the loader array for a LUT folder's bitplane count. */
+int bpc_lut_entries(int passes, int levels, int max_bitplane);
+
+int bpc_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BPC_PACO_H */

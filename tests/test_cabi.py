@@ -1,0 +1,101 @@
+"""The C ABI library: loads, exports every function include/bpc_paco.h
+declares, validates arguments, and its host LUT loader (no GPU calls)."""
+import ctypes
+import os
+import re
+import tempfile
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, ROOT, lut_folder
+
+
+def header_functions():
+    text = open(os.path.join(ROOT, "include", "bpc_paco.h")).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    text = "\n".join(l for l in text.splitlines() if not l.lstrip().startswith("#"))
+    decl = r"^\s*(?:const\s+)?(?:void|int|char)\s*\**\s*([A-Za-z_]\w*)\s*\([^;{]*\)\s*;"
+    return sorted(set(re.findall(decl, text, flags=re.M)))
+
+
+def test_exports_every_declared_symbol(bpc):
+    names = header_functions()
+    assert {"CUDA_BPC", "load_LUTs", "bpc_encode_device", "bpc_decode_device"} <= set(names)
+    L = bpc.lib()
+    for n in names:
+        assert hasattr(L, n), n
+    assert set(bpc.EXPORTS) <= set(names)
+
+
+def test_mode_validation(bpc):
+    assert bpc.get_mode() == (2, 5, 64)
+    assert bpc.lib().bpc_set_mode(4, 5, 64) == bpc.ERR_ARG
+    assert bpc.lib().bpc_set_mode(2, 5, 48) == bpc.ERR_ARG
+    bpc.set_mode(3, 6, 32)
+    assert bpc.get_mode() == (3, 6, 32)
+    bpc.set_mode(2, 5, 64)
+
+
+def test_status_strings(bpc):
+    assert bpc.status_string(0) == "ok"
+    assert "overflow" in bpc.status_string(bpc.ST_SLOT_OVERFLOW)
+    assert "LUT" in bpc.status_string(bpc.ERR_PARSE)
+
+
+@pytest.mark.parametrize("passes", [2, 3])
+def test_host_lut_loader_matches_layout(bpc, passes):
+    got = bpc.load_luts_host(lut_folder(passes), passes, 5)
+    want = np.load(os.path.join(GOLDEN, f"lut_naive_{passes}pass_L5.npy"))
+    np.testing.assert_array_equal(got, want)
+
+
+@pytest.mark.parametrize("levels", [1, 2, 3, 4, 6, 7])
+@pytest.mark.parametrize("passes", [2, 3])
+def test_host_lut_loader_other_levels_matches_oracle(bpc, oracle_mod, passes, levels):
+    """DWT_LEVELS != 5 with the shipped 16-group files: truncated at the
+    allocation (fewer levels) or zero-filled (more levels)."""
+    np.testing.assert_array_equal(bpc.load_luts_host(lut_folder(passes), passes, levels),
+                                  oracle_mod.load_luts(lut_folder(passes), passes, levels))
+
+
+def test_lut_fill_rule(bpc, oracle_mod):
+    """A group that lists planes 0..2 only: the fill writes 64 from entry
+    2*N + 1 onward (overwriting contexts 1..N-1 of plane 2), the last group
+    is not filled (main_example.cu:315-319)."""
+    with tempfile.TemporaryDirectory() as d:
+        rows = {"ref.txt": 1, "sig.txt": 9, "sign.txt": 4}
+        for name, n in rows.items():
+            with open(os.path.join(d, name), "w") as f:
+                for g in range(2):
+                    for bp in range(3):
+                        vals = " ".join(str(10 + g * 20 + bp * 3 + k) for k in range(n))
+                        f.write(f"0 {g} {bp} : {vals}\n")
+        got = bpc.load_luts_host(d + "/", 2, 1)
+        want = oracle_mod.load_luts(d + "/", 2, 1)
+        np.testing.assert_array_equal(got, want)
+        mb = 3
+        sig0 = 3 * mb * 1 * 1 + mb  # ref section size for levels = 1
+        assert got[sig0 + 2 * 9] == 10 + 6  # plane 2, context 0 kept
+        assert (got[sig0 + 2 * 9 + 1: sig0 + 3 * 9] == 64).all()  # contexts 1..8 overwritten
+        assert got[mb] == 30  # group 1, plane 0 of ref
+
+
+def test_lut_loader_errors(bpc):
+    n = ctypes.c_int()
+    assert bpc.lib().bpc_load_luts_host(b"/nonexistent/", 2, 5, None, 0, ctypes.byref(n)) == bpc.ERR_FILE
+    with tempfile.TemporaryDirectory() as d:
+        for name in ("ref.txt", "sig.txt", "sign.txt"):
+            open(os.path.join(d, name), "w").write("0 0 0 : 1 2\n0 0 x\n")
+        assert bpc.lib().bpc_load_luts_host((d + "/").encode(), 2, 5, None, 0, ctypes.byref(n)) == bpc.ERR_PARSE
+
+
+def test_device_entry_points_reject_bad_geometry(bpc):
+    """Argument checks happen before any CUDA call."""
+    vp = ctypes.c_void_p
+    L = bpc.lib()
+    for X, Y, cb in ((100, 64, 64), (64, 64, 48), (0, 64, 64)):
+        rc = L.bpc_encode_device(vp(16), vp(16), X, Y, vp(16), 3360, 2, 5, cb, None, None, 0, None)
+        assert rc == bpc.ERR_ARG
+    assert L.bpc_decode_device(vp(16), vp(16), 64, 64, None, 3360, 2, 5, 64, None, None, 0, None) == bpc.ERR_ARG
+    assert L.bpc_encode_device(vp(16), vp(16), 64, 64, vp(16), 3360, 4, 5, 64, None, None, 0, None) == bpc.ERR_ARG

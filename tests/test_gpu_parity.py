@@ -1,0 +1,147 @@
+"""Parity of the sm_100a coder with the oracle: every stream word and every
+decoded coefficient bit-exact, called through the C ABI."""
+import numpy as np
+import pytest
+
+import bpc_synth
+from conftest import lut_folder
+
+pytestmark = pytest.mark.gpu
+
+
+def synth(side, levels, seed, amp=20.0, nrect=30):
+    return bpc_synth.synthetic_coefficients(side, levels, seed, amp=amp, nrect=nrect)
+
+
+def check_roundtrip(bpc, oracle_mod, img, passes, levels, cb, lut_np=None):
+    """Encode + decode on the GPU through bpc_code_host; compare with the oracle."""
+    lut = bpc.DeviceLut(lut_folder(passes), passes, levels)
+    try:
+        if lut_np is None:
+            lut_np = oracle_mod.load_luts(lut_folder(passes), passes, levels)
+        want, wst = oracle_mod.encode(img, lut_np, passes, levels, cb, with_status=True)
+        got, st = bpc.encode_host(img, lut, cb)
+        bad = np.nonzero(got != want)[0]
+        assert bad.size == 0, f"first stream mismatch at {bad[:8]} (slot {bad[0] // (cb * cb)})"
+        assert st == int(np.bitwise_or.reduce(wst))
+        dec, dst = bpc.decode_host(got, img.shape, lut, cb)
+        wdec, _ = oracle_mod.decode(want, img.shape, lut_np, passes, levels, cb, with_status=True)
+        np.testing.assert_array_equal(dec, wdec)
+        ok = np.nonzero(wst == 0)[0]
+        ncbx = img.shape[1] // cb
+        for k in ok[:: max(1, len(ok) // 64)]:
+            y0, x0 = (k // ncbx) * cb, (k % ncbx) * cb
+            np.testing.assert_array_equal(dec[y0:y0 + cb, x0:x0 + cb], img[y0:y0 + cb, x0:x0 + cb])
+        return got, st
+    finally:
+        lut.close()
+
+
+@pytest.mark.parametrize("passes", [2, 3])
+def test_small_synthetic(bpc, oracle_mod, passes):
+    img = synth(256, 5, 3, amp=40)
+    _, st = check_roundtrip(bpc, oracle_mod, img, passes, 5, 64)
+    assert st == 0
+
+
+@pytest.mark.parametrize("passes", [2, 3])
+def test_sample_subset(bpc, oracle_mod, sample_subset, passes):
+    """The reference's sample codeblocks (MSB up to 12) at their positions;
+    the other codeblocks are all-zero (MSB = 32)."""
+    check_roundtrip(bpc, oracle_mod, sample_subset, passes, 5, 64)
+
+
+def test_config1_2048_2pass(bpc, oracle_mod):
+    img = synth(2048, 5, 1, amp=20, nrect=30)
+    check_roundtrip(bpc, oracle_mod, img, 2, 5, 64)
+
+
+def test_config2_4096_3pass(bpc, oracle_mod):
+    img = synth(4096, 5, 2, amp=40, nrect=60)
+    check_roundtrip(bpc, oracle_mod, img, 3, 5, 64)
+
+
+@pytest.mark.parametrize("passes", [2, 3])
+@pytest.mark.parametrize("levels", [3, 6])
+def test_cb32(bpc, oracle_mod, passes, levels):
+    img = synth(512, levels, 10 + levels, amp=30)
+    check_roundtrip(bpc, oracle_mod, img, passes, levels, 32)
+
+
+@pytest.mark.parametrize("passes", [2, 3])
+def test_straddling_codeblocks(bpc, oracle_mod, passes):
+    """3072 >> 5 = 96 is not a multiple of 64: codeblocks straddle subbands
+    and lanes of one warp use different LUT groups."""
+    img = synth(3072, 5, 21, amp=30)[:1024, :]
+    check_roundtrip(bpc, oracle_mod, np.ascontiguousarray(img), passes, 5, 64)
+
+
+@pytest.mark.parametrize("passes", [2, 3])
+def test_all_zero_and_sparse(bpc, oracle_mod, passes):
+    img = np.zeros((512, 512), np.int32)
+    img[70, 3] = -1
+    img[300, 301] = 5
+    img[511, 511] = 1 << 20
+    check_roundtrip(bpc, oracle_mod, img, passes, 5, 64)
+
+
+@pytest.mark.parametrize("passes", [2, 3])
+def test_laplacian_plane15(bpc, oracle_mod, passes):
+    """Every magnitude plane up to 15 populated: LL codeblocks read LUT
+    entries past the loader's array (zero padding)."""
+    img = bpc_synth.laplacian_coefficients(512, 5, 4)
+    img[0, 0] = 40000
+    check_roundtrip(bpc, oracle_mod, img, passes, 5, 64)
+
+
+def test_slot_overflow(bpc, oracle_mod):
+    rng = np.random.default_rng(3)
+    img = rng.integers(-(1 << 15), 1 << 15, size=(128, 128)).astype(np.int32)
+    _, st = check_roundtrip(bpc, oracle_mod, img, 2, 5, 64)
+    assert st & bpc.ST_SLOT_OVERFLOW
+
+
+def test_device_api_and_persistent_grid(bpc, oracle_mod):
+    import torch
+    img = synth(1024, 5, 8, amp=40)
+    lut_np = oracle_mod.load_luts(lut_folder(3), 3, 5)
+    want = oracle_mod.encode(img, lut_np, 3, 5, 64)
+    lut = bpc.DeviceLut(lut_folder(3), 3, 5)
+    try:
+        d_img = torch.from_numpy(img).cuda()
+        outs = []
+        for grid in (0, 37, 148):
+            s = torch.full((img.size,), 12345, dtype=torch.int32, device="cuda")
+            st = torch.zeros(1, dtype=torch.int32, device="cuda")
+            cnt = torch.zeros(256, dtype=torch.int32, device="cuda")
+            bpc.encode_device(d_img, s, lut, 64, st, cnt, grid)
+            torch.cuda.synchronize()
+            got = s.cpu().numpy()
+            np.testing.assert_array_equal(got, want)
+            assert st.item() == 0
+            used = (want.reshape(-1, 4096)[:, 1:] != -1).sum(1)
+            np.testing.assert_array_equal(cnt.cpu().numpy(), used)
+            dec = torch.empty_like(d_img)
+            bpc.decode_device(s, dec, lut, 64, st, None, grid)
+            torch.cuda.synchronize()
+            np.testing.assert_array_equal(dec.cpu().numpy(), img)
+            outs.append(got)
+    finally:
+        lut.close()
+
+
+def test_drop_in_flow(bpc, oracle_mod, sample_subset):
+    """main_example.cu:498-532: load_LUTs, CUDA_BPC(CODE), load_LUTs again
+    (CUDA_BPC frees it), CUDA_BPC(DECODE), compare."""
+    for passes in (2, 3):
+        bpc.set_mode(passes, 5, 64)
+        h = sample_subset.copy().reshape(-1)
+        lut = bpc.load_LUTs(lut_folder(passes))
+        assert lut
+        assert bpc.CUDA_BPC(bpc.CODE, h, 2048, 2048, lut) == 0
+        want = oracle_mod.encode(sample_subset, oracle_mod.load_luts(lut_folder(passes), passes, 5), passes)
+        np.testing.assert_array_equal(h, want)
+        lut = bpc.load_LUTs(lut_folder(passes))
+        assert bpc.CUDA_BPC(bpc.DECODE, h, 2048, 2048, lut) == 0
+        np.testing.assert_array_equal(h.reshape(2048, 2048), sample_subset)
+    bpc.set_mode(2, 5, 64)
