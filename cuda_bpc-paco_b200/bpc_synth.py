@@ -64,7 +64,7 @@ def make_image(side: int, seed: int, amp: float = 20.0, nrect: int = 30, height:
         h = int(rng.integers(max(2, H // 64), max(3, H // 5)))
         x0 = int(rng.integers(0, W - w))
         y0 = int(rng.integers(0, H - h))
-        img[y0:y0 + h, x0:x0 + w] += rng.uniform(-160.0, 160.0)
+        img[y0:y0 + h, x0:x0 + w] += rng.uniform(-80.0, 80.0)
     return np.clip(np.rint(img), 0, 255).astype(np.uint8)
 
 
