@@ -234,6 +234,16 @@ def run_ours(args, c):
         t_step = float(t.item())
     value = 2 * N * world / t_step / 1e9
 
+    if args.no_e2e:
+        lut.close()
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "value": value, "unit": "Gcoeff/s", "partial": "no e2e",
+                              "encode_gcoeffs": N / (te / args.steps) / 1e9,
+                              "decode_gcoeffs": N / (td / args.steps) / 1e9}))
+        if dist:
+            tdist.destroy_process_group()
+        return
+
     # e2e through the C ABI with pinned host buffers (copies inside the timed region)
     h = torch.empty(N, dtype=torch.int32, pin_memory=True)
     hn = h.numpy()
@@ -301,6 +311,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="cfg2", choices=sorted(CONFIGS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true", help="kernel timing only (profiling runs)")
     args = ap.parse_args()
     c = CONFIGS[args.config]
     if args.impl == "reference":

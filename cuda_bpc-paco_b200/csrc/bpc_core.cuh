@@ -17,10 +17,12 @@
 // copies of the two neighbour columns (lane-1's right column, lane+1's left
 // column) that are kept current with one ballot per step that changes them.
 // A context is a popcount of a 9-bit neighbourhood gathered from three 3-row
-// windows; there are no per-coefficient shuffles.  Magnitudes live in shared
-// memory ([row][column][lane], conflict-free), the LUT in shared memory as
-// bytes, the decoder's codewords in a per-codeblock shared-memory ring that is
-// refilled with 16-byte loads as the codeword counter advances.
+// windows; there are no per-coefficient shuffles.  Magnitudes are held as
+// bitplanes (one 64-bit row mask per plane and column) in a per-thread array
+// built with an in-register 32x32 bit transpose; the decoder collects decoded
+// planes the same way and transposes them back at the end.  No shared memory
+// is reserved per codeblock except the decoder's codeword ring, so a CTA of 4
+// warps fits 7 times per SM.  The LUT sits in shared memory as bytes.
 //
 // The code is written against a small warp interface W (lane id, ballot, any,
 // shuffles, syncwarp) so the same source runs as a CUDA kernel (bpc_kernels.cu).
@@ -92,7 +94,6 @@ struct Geo {
     static constexpr int CAP = CBS * CBS;                // slot size in ints
     static constexpr int RING = CBS == 64 ? 512 : 256;   // decoder ring per codeblock
     static constexpr int CHUNK = RING / 2;               // refill size
-    static constexpr int MAG_WORDS = CBS * 2 * 32;       // per warp
     static constexpr int RING_WORDS = RING * NG;         // per warp
     static constexpr uint64_t ROWS = CBS == 64 ? ~0ull : 0xffffffffull;
 };
@@ -122,6 +123,21 @@ BPC_FI int clz32(uint32_t x) {
 #else
     return x ? __builtin_clz(x) : 32;
 #endif
+}
+
+// In-register transpose of a 32x32 bit matrix, LSB first: afterwards bit r of
+// a[c] is what bit c of a[r] was.  (Recursive block swap; 5 x 16 exchanges.)
+BPC_FI void transpose32(uint32_t a[32]) {
+    uint32_t m = 0x0000FFFFu;
+#pragma unroll
+    for (int j = 16; j; j >>= 1, m ^= m << j) {
+#pragma unroll
+        for (int k = 0; k < 32; k = (k + j + 1) & ~j) {
+            const uint32_t t = ((a[k] >> j) ^ a[k + j]) & m;
+            a[k + j] ^= t;
+            a[k] ^= t << j;
+        }
+    }
 }
 
 struct Lane {
@@ -158,19 +174,23 @@ BPC_FI uint64_t shfl_down64(W &w, uint64_t v) {
 template <int PASSES, int CBS, bool ENC, class W>
 struct Coder {
     using G = Geo<CBS>;
+    static constexpr int NH = CBS / 32;  // 32-row halves per column
     W &w;
     const Params &p;
     Lane s;
-    uint32_t *mag;       // per warp [row][col][lane]
     uint32_t *ring;      // per codeblock (decoder)
     const uint8_t *tab;  // LUT bytes
     const int32_t *slot_in;
     int32_t *slot_out;
     int lane, gl, g, msb;
+    int top;  // highest stored bitplane (-1: none)
     uint32_t gmask, ltmask;
+    uint64_t B[2];  // encoder: magnitude bits of the current plane; decoder: decoded 1-bits
+    int sig_base, sign_base;  // LUT byte indices of the current plane and pass
+    // bitplanes, [plane][col0 rows 0-31, col0 rows 32-63, col1 rows 0-31, col1 rows 32-63]
+    uint32_t planes[28][4];
 
-    BPC_FI Coder(W &w_, const Params &p_, uint32_t *mag_, uint32_t *ring_all, const uint8_t *tab_)
-        : w(w_), p(p_), mag(mag_), tab(tab_) {
+    BPC_FI Coder(W &w_, const Params &p_, uint32_t *ring_all, const uint8_t *tab_) : w(w_), p(p_), tab(tab_) {
         lane = w.lane();
         gl = lane % G::NL;
         const int grp = lane / G::NL;
@@ -270,8 +290,6 @@ struct Coder {
         }
     }
 
-    BPC_FI uint32_t &magw(int i, int c) { return mag[(i * 2 + c) * 32 + lane]; }
-
     // Decoder reconstruction: the reference ORs a plane mask 3 << b into the
     // coefficient (:1038-1083); every bit it sets is later replaced by the
     // decoded bit, so the output holds exactly the decoded bits -- except for
@@ -284,10 +302,34 @@ struct Coder {
     // constants.  Planes >= 28 are only visited by all-zero codeblocks (MSB 32).
     template <int PK>
     BPC_FI uint32_t data_bit(int i, int c, int b) {
-        if (b <= 27) return (magw(i, c) >> b) & 1u;
+        if (b <= 27) return (uint32_t)(B[c] >> i) & 1u;
         if (PK == PK_CP) return b == 29 ? 1u : 0u;
         if (PK == PK_MRP) return (b == 28 || b == 30) ? 1u : 0u;
         return 0u;
+    }
+
+    // plane registers: encoder loads the magnitude bits, decoder clears
+    BPC_FI void plane_begin(int b) {
+        if (ENC) {
+            if (b <= top) {
+                const uint32_t *q = planes[b];
+                B[0] = (uint64_t)q[0] | ((uint64_t)q[1] << 32);
+                B[1] = (uint64_t)q[2] | ((uint64_t)q[3] << 32);
+            } else {
+                B[0] = B[1] = 0ull;
+            }
+        } else {
+            B[0] = B[1] = 0ull;
+        }
+    }
+    BPC_FI void plane_end(int b) {
+        if (!ENC && b <= 27 && keep_bit(b)) {
+            uint32_t *q = planes[b];
+            q[0] = (uint32_t)B[0];
+            q[1] = (uint32_t)(B[0] >> 32);
+            q[2] = (uint32_t)B[1];
+            q[3] = (uint32_t)(B[1] >> 32);
+        }
     }
 
     // ------------------------------------------------------- context steps
@@ -308,9 +350,7 @@ struct Coder {
             }
         }
         const int ctx = popc32(nbh);
-        const int gb = g + b;
-        const int off = PK == PK_CP ? p.cp_off : 0;
-        const uint32_t P = coded ? tab[off + p.a_sig + gb * 9 + ctx] : 0u;
+        const uint32_t P = coded ? tab[sig_base + ctx] : 0u;
         uint32_t sym;
         if (ENC) {
             sym = coded ? data_bit<PK>(i, c, b) : 0u;
@@ -323,7 +363,7 @@ struct Coder {
         if (ns) {
             s.S[c] |= bit;
             if (PK == PK_CP) s.R[c] |= bit;
-            if (!ENC && keep_bit(b)) magw(i, c) |= 1u << b;
+            if (!ENC) B[c] |= bit;
         }
         if (!w.any(ns)) return;
         // sign call (Compute_Sign_Context :214-226 over u, l, r, b)
@@ -336,7 +376,7 @@ struct Coder {
         const int v = us * (1 - 2 * un) + bs * (1 - 2 * bn);
         const int hc = h == 0 ? 0 : (h > 0 ? 1 : 2), vc = v == 0 ? 0 : (v > 0 ? 1 : 2);
         const int sctx = (int)((kSignTab >> (3 * (hc * 3 + vc))) & 7u);
-        const uint32_t P2 = ns ? tab[off + p.a_sign + gb * 4 + (sctx >> 1)] : 0u;
+        const uint32_t P2 = ns ? tab[sign_base + (sctx >> 1)] : 0u;
         uint32_t neg;
         if (ENC) {
             neg = (uint32_t)((s.N[c] >> i) & 1);
@@ -363,6 +403,9 @@ struct Coder {
 
     template <int PK>
     BPC_FI void ctx_pass(int b, bool act) {
+        const int off = PK == PK_CP ? p.cp_off : 0;
+        sig_base = off + p.a_sig + (g + b) * 9;
+        sign_base = off + p.a_sign + (g + b) * 4;
         const uint64_t c0 = act ? (PK == PK_SPP ? ~s.S[0] : s.C[0]) : 0ull;
         const uint64_t c1 = act ? (PK == PK_SPP ? ~s.S[1] : s.C[1]) : 0ull;
         uint64_t U = warp_or64(w, (c0 | c1) & G::ROWS);
@@ -384,7 +427,7 @@ struct Coder {
         } else {
             ring_ensure();
             const uint32_t sym = ac_dec(cand, P);
-            if (cand && sym && b <= 27 && keep_bit(b)) magw(i, c) |= 1u << b;
+            if (cand && sym && b <= 27) B[c] |= 1ull << i;
         }
     }
 
@@ -429,20 +472,19 @@ struct Coder {
         s.has_resv = 0;
         s.status = 0;
         const size_t cap = (size_t)G::CAP;
+        const int32_t *src = p.in + (size_t)y0 * (size_t)p.X + (size_t)x;
         msb = -1;
+        top = -1;
         if (ENC) {
             slot_out = p.out + (ok ? (size_t)cb * cap : 0);
-            // Read_Coefficients :14-44 + Find_MSB :114-161
+            // Read_Coefficients :14-44 + Find_MSB :114-161: signs and OR
             uint32_t mx = 0;
             if (ok) {
-                const int32_t *src = p.in + (size_t)y0 * (size_t)p.X + (size_t)x;
                 for (int i = 0; i < CBS; i++) {
                     int32_t v0, v1;
                     w.load2(src + (size_t)i * (size_t)p.X, v0, v1);
                     const uint32_t m0 = v0 < 0 ? 0u - (uint32_t)v0 : (uint32_t)v0;
                     const uint32_t m1 = v1 < 0 ? 0u - (uint32_t)v1 : (uint32_t)v1;
-                    magw(i, 0) = m0;
-                    magw(i, 1) = m1;
                     s.N[0] |= (uint64_t)(v0 < 0) << i;
                     s.N[1] |= (uint64_t)(v1 < 0) << i;
                     mx |= m0 | m1;
@@ -453,6 +495,24 @@ struct Coder {
             if (ok) {
                 msb = mx ? 31 - clz32(mx) : 32;
                 if (gl == 0) slot_out[0] = msb;  // :1155
+                // bitplanes 0..min(MSB, 27): transpose 32 rows x 32 bits at a time
+                top = msb <= 27 ? msb : -1;
+                if (top >= 0) {
+#pragma unroll 1
+                    for (int q = 0; q < 2 * NH; q++) {
+                        const int c = q / NH, h = q % NH;
+                        uint32_t a[32];
+#pragma unroll
+                        for (int r = 0; r < 32; r++) {
+                            const int32_t v = w.load1(src + (size_t)(h * 32 + r) * (size_t)p.X + c);
+                            a[r] = v < 0 ? 0u - (uint32_t)v : (uint32_t)v;
+                        }
+                        transpose32(a);
+#pragma unroll
+                        for (int k = 0; k < 28; k++)
+                            if (k <= top) planes[k][c * 2 + h] = a[k];
+                    }
+                }
             }
             // neighbour sign columns are data: lane-1's right, lane+1's left
             const uint64_t up = shfl_up64(w, s.N[1]), dn = shfl_down64(w, s.N[0]);
@@ -460,7 +520,6 @@ struct Coder {
             s.XNR = gl < G::NL - 1 ? dn : 0ull;
         } else {
             slot_in = p.in + (ok ? (size_t)cb * cap : 0);
-            for (int i = 0; i < CBS; i++) magw(i, 0) = magw(i, 1) = 0u;
             if (ok) {
                 ring_load(0u, G::RING);
                 s.ring_hi = G::RING;
@@ -488,11 +547,13 @@ struct Coder {
             // only, planes below run SPP, MRP, CP (:986-1018).
             const bool full = PASSES == 2 ? b <= msb : b < msb;
             const bool first_cp = PASSES == 3 && b == msb;
+            plane_begin(b);
             if (w.any(full)) {
                 ctx_pass<PK_SPP>(b, full);
                 mrp_pass(b, full);
             }
             if (PASSES == 3 && w.any(full || first_cp)) ctx_pass<PK_CP>(b, full || first_cp);
+            if (b <= msb) plane_end(b);
         }
         if (ENC) {
             if (ok) {
@@ -507,13 +568,22 @@ struct Coder {
                 if (s.cnt + 1u > (uint32_t)G::CAP) s.status |= ST_OVERFLOW;
             }
         } else if (ok) {
-            // Write_Coefficients :46-63
+            // Write_Coefficients :46-63: planes back to magnitudes
+            top = msb == 32 ? 0 : msb;
             int32_t *dst = p.out + (size_t)y0 * (size_t)p.X + (size_t)x;
-            for (int i = 0; i < CBS; i++) {
-                const int32_t m0 = (int32_t)magw(i, 0), m1 = (int32_t)magw(i, 1);
-                const int32_t v0 = ((s.N[0] >> i) & 1) ? -m0 : m0;
-                const int32_t v1 = ((s.N[1] >> i) & 1) ? -m1 : m1;
-                w.store2(dst + (size_t)i * (size_t)p.X, v0, v1);
+#pragma unroll 1
+            for (int q = 0; q < 2 * NH; q++) {
+                const int c = q / NH, h = q % NH;
+                uint32_t a[32];
+#pragma unroll
+                for (int k = 0; k < 32; k++) a[k] = (k < 28 && k <= top) ? planes[k < 28 ? k : 0][c * 2 + h] : 0u;
+                transpose32(a);
+                const uint64_t neg = s.N[c] >> (32 * h);
+#pragma unroll
+                for (int r = 0; r < 32; r++) {
+                    const int32_t m = (int32_t)a[r];
+                    w.store1(dst + (size_t)(h * 32 + r) * (size_t)p.X + c, ((neg >> r) & 1) ? -m : m);
+                }
             }
         }
         if (ok && p.counts && gl == 0) p.counts[cb] = (int)s.cnt;

@@ -4,6 +4,8 @@
 // kWarps warps stages the LUT once into shared memory as bytes and then walks
 // codeblocks grid-stride, so the same kernel serves the plain one-image launch
 // (grid = ceil(ncb / kWarps)) and a persistent launch (grid = k * 148).
+// kMinCtas CTAs per SM (28 warps) keep every codeblock of a 4096x4096 image
+// resident in one wave.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -26,6 +28,8 @@ struct GpuWarp {
         a = v.x;
         b = v.y;
     }
+    __device__ __forceinline__ int32_t load1(const int32_t *p) { return __ldg(p); }
+    __device__ __forceinline__ void store1(int32_t *p, int32_t a) { *p = a; }
     __device__ __forceinline__ void store2(int32_t *p, int32_t a, int32_t b) {
         *reinterpret_cast<int2 *>(p) = make_int2(a, b);
     }
@@ -40,7 +44,7 @@ struct GpuWarp {
 };
 
 template <int PASSES, int CBS, bool ENC>
-__global__ void __launch_bounds__(kWarps * 32) k_bpc(Params p) {
+__global__ void __launch_bounds__(kWarps * 32, kMinCtas) k_bpc(Params p) {
     using G = Geo<CBS>;
     extern __shared__ __align__(16) unsigned char smem[];
     uint8_t *tab = smem;
@@ -56,13 +60,11 @@ __global__ void __launch_bounds__(kWarps * 32) k_bpc(Params p) {
     if (bad && p.status) atomicOr(p.status, ST_LUT_RANGE);
     __syncthreads();
     const int warp = (int)(threadIdx.x >> 5);
-    uint32_t *words = reinterpret_cast<uint32_t *>(smem + p.tab_n);
-    uint32_t *mag = words + warp * G::MAG_WORDS;
-    uint32_t *ring = words + kWarps * G::MAG_WORDS + warp * G::RING_WORDS;
+    uint32_t *ring = reinterpret_cast<uint32_t *>(smem + p.tab_n) + warp * G::RING_WORDS;
     GpuWarp w;
     const int stride = (int)gridDim.x * kWarps * G::NG;
     for (int base = ((int)blockIdx.x * kWarps + warp) * G::NG; base < p.ncb; base += stride) {
-        Coder<PASSES, CBS, ENC, GpuWarp> cd(w, p, mag, ring, tab);
+        Coder<PASSES, CBS, ENC, GpuWarp> cd(w, p, ring, tab);
         cd.run(base);
     }
 }
@@ -70,7 +72,7 @@ __global__ void __launch_bounds__(kWarps * 32) k_bpc(Params p) {
 template <int PASSES, int CBS, bool ENC>
 static size_t smem_bytes(const Params &p) {
     using G = Geo<CBS>;
-    return (size_t)p.tab_n + (size_t)kWarps * 4u * (size_t)(G::MAG_WORDS + (ENC ? 0 : G::RING_WORDS));
+    return (size_t)p.tab_n + (size_t)kWarps * 4u * (size_t)(ENC ? 0 : G::RING_WORDS);
 }
 
 template <int PASSES, int CBS, bool ENC>

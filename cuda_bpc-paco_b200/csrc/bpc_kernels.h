@@ -7,7 +7,8 @@
 
 namespace bpc {
 
-constexpr int kWarps = 4;  // warps (codeblocks) per CTA
+constexpr int kWarps = 4;    // warps (codeblocks) per CTA
+constexpr int kMinCtas = 7;  // CTAs per SM the register budget is sized for
 
 // Launch the encoder (enc) or decoder over p.ncb codeblocks.  grid <= 0 picks
 // one CTA per kWarps codeblocks; a positive grid runs persistent CTAs that
