@@ -140,6 +140,38 @@ BPC_FI void transpose32(uint32_t a[32]) {
     }
 }
 
+BPC_FI uint32_t bit64(uint64_t m, int i) { return (uint32_t)(m >> i) & 1u; }
+
+// Interleave the low 16 bits of a (even positions) and b (odd positions):
+// row j of the left column -> bit 2j, of the right column -> bit 2j+1, which
+// is the scan order of one lane's two columns.
+BPC_FI uint32_t spread16(uint32_t x) {
+    x &= 0xFFFFu;
+    x = (x | (x << 8)) & 0x00FF00FFu;
+    x = (x | (x << 4)) & 0x0F0F0F0Fu;
+    x = (x | (x << 2)) & 0x33333333u;
+    x = (x | (x << 1)) & 0x55555555u;
+    return x;
+}
+BPC_FI uint32_t zip16(uint64_t l, uint64_t r, int q) {
+    return spread16((uint32_t)(l >> (16 * q))) | (spread16((uint32_t)(r >> (16 * q))) << 1);
+}
+
+// Per-row count (0..8) of eight 64-bit row masks, as four bit slices
+// (carry-save adder tree; bit i of slice k = bit k of the count at row i).
+BPC_FI void count8(const uint64_t x[8], uint64_t &c0, uint64_t &c1, uint64_t &c2, uint64_t &c3) {
+    const uint64_t s1 = x[0] ^ x[1] ^ x[2], k1 = (x[0] & x[1]) | (x[2] & (x[0] ^ x[1]));
+    const uint64_t s2 = x[3] ^ x[4] ^ x[5], k2 = (x[3] & x[4]) | (x[5] & (x[3] ^ x[4]));
+    const uint64_t s3 = x[6] ^ x[7], k3 = x[6] & x[7];
+    c0 = s1 ^ s2 ^ s3;
+    const uint64_t k4 = (s1 & s2) | (s3 & (s1 ^ s2));  // weight 2
+    const uint64_t t = k1 ^ k2 ^ k3, k5 = (k1 & k2) | (k3 & (k1 ^ k2));  // weight 2 / 4
+    c1 = t ^ k4;
+    const uint64_t k6 = t & k4;  // weight 4
+    c2 = k5 ^ k6;
+    c3 = k5 & k6;
+}
+
 struct Lane {
     uint64_t S[2], R[2], C[2], N[2];
     uint64_t XL, XR, XNL, XNR;
@@ -148,6 +180,11 @@ struct Lane {
     uint32_t ring_hi;  // decoder: slot words [ring_hi - RING, ring_hi) are in the ring
     int has_resv;
     int status;
+    // encoder: slot of the open codeword (-1: reserved in the current chunk,
+    // slot not ranked yet) and the chunk's event list length
+    int open_slot;
+    int cur_ev;
+    int nev;
 };
 
 template <class W>
@@ -187,10 +224,24 @@ struct Coder {
     uint32_t gmask, ltmask;
     uint64_t B[2];  // encoder: magnitude bits of the current plane; decoder: decoded 1-bits
     int sig_base, sign_base;  // LUT byte indices of the current plane and pass
+    // encoder, per pass: coded (K), symbol-1 (Y) and newly significant (NS)
+    // masks, neighbour columns' significance at pass start and new in pass
+    uint64_t K[2], Y[2], NS[2], XLS, XRS, XLN, XRN;
+    uint64_t cs[2][4];  // context bit slices per column
+    uint32_t *evmask;   // per warp, 256 keys: lanes with a reservation event
+    uint32_t *pfx;      // per warp, 256 keys: events before the key (ranking)
+    uint8_t *ev_key;    // this lane's events of the pass: key, finished codeword
+    uint32_t *ev_val;
     // bitplanes, [plane][col0 rows 0-31, col0 rows 32-63, col1 rows 0-31, col1 rows 32-63]
-    uint32_t planes[28][4];
+    // (per-thread arrays owned by the caller: an array indexed at run time
+    // inside this struct would keep the whole struct out of registers)
+    uint32_t (*planes)[4];
 
-    BPC_FI Coder(W &w_, const Params &p_, uint32_t *ring_all, const uint8_t *tab_) : w(w_), p(p_), tab(tab_) {
+    BPC_FI Coder(W &w_, const Params &p_, uint32_t *ring_all, const uint8_t *tab_, uint32_t (*planes_)[4],
+                 uint8_t *ev_key_, uint32_t *ev_val_)
+        : w(w_), p(p_), tab(tab_), planes(planes_), ev_key(ev_key_), ev_val(ev_val_) {
+        evmask = ring_all;
+        pfx = ring_all + 256;
         lane = w.lane();
         gl = lane % G::NL;
         const int grp = lane / G::NL;
@@ -446,6 +497,278 @@ struct Coder {
         }
     }
 
+    // ---------------------------------------------------- encoder, decoupled
+    // The encoder knows every data bit up front, so per pass it computes, for
+    // all rows at once, which coefficients are coded (K), which code a 1 (Y),
+    // which become significant (NS) and their contexts from time-accurate
+    // neighbour significance (earlier in scan order: start of pass | NS; later:
+    // start of pass).  Each lane then runs its arithmetic coder over its own
+    // coded symbols only.  A reservation (:268-279) is recorded as an event
+    // keyed by (row, column, phase) inside a 16-row chunk; after the chunk the
+    // warp ranks all events by (key, lane) -- the reference's lockstep order --
+    // and the codewords go to their slots.
+
+    // Arithmetic_encoder :261-295 for this lane; reservation -> event
+    BPC_FI void enc_symbol(uint32_t sym, uint32_t P, int key) {
+        if (s.size == 0) {
+            ev_key[s.nev] = (uint8_t)key;
+            ev_val[s.nev] = 0u;
+            s.cur_ev = s.nev;
+            s.nev++;
+            w.smem_or(&evmask[key], 1u << lane);
+            s.has_resv = 1;
+            s.lower = 0;
+            s.size = 0xFFFFu;
+        }
+        const uint32_t t = ((s.size * P) >> 7) + sym;
+        if (sym) {
+            s.size -= t;
+            s.lower += t;
+        } else {
+            s.size = t;
+        }
+        if (s.size == 0) {
+            if (s.cur_ev >= 0)
+                ev_val[s.cur_ev] = s.lower;
+            else if (s.open_slot < G::CAP)
+                slot_out[s.open_slot] = (int32_t)s.lower;
+            else
+                s.status |= ST_OVERFLOW;
+        }
+    }
+
+    // Rank the pass's events by (key, lane) and store completed codewords.
+    BPC_FI void enc_rank() {
+        if (!w.any(s.nev > 0)) return;
+        w.sync();
+        uint32_t c[8], v = 0;
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+            const uint32_t m = evmask[8 * lane + k];
+            c[k] = G::NL == 32 ? (uint32_t)popc32(m)
+                               : ((uint32_t)popc32(m & 0xFFFFu) | ((uint32_t)popc32(m >> 16) << 16));
+            v += c[k];
+        }
+        const uint32_t own = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t t = w.shfl_up(v, o);
+            if (lane >= o) v += t;
+        }
+        uint32_t run = v - own;
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+            pfx[8 * lane + k] = run;
+            run += c[k];
+        }
+        const uint32_t tot = w.shfl_idx(v, 31);
+        w.sync();
+        const int sh = G::NL == 32 ? 0 : 16 * (lane / G::NL);
+        const uint32_t hm = G::NL == 32 ? 0xFFFFFFFFu : 0xFFFFu;
+        for (int e = 0; e < s.nev; e++) {
+            const int key = ev_key[e];
+            const uint32_t slot = 1u + s.cnt + ((pfx[key] >> sh) & hm) + (uint32_t)popc32(evmask[key] & ltmask & gmask);
+            if (e < s.nev - 1 || s.size == 0) {
+                if (slot < (uint32_t)G::CAP)
+                    slot_out[slot] = (int32_t)ev_val[e];
+                else
+                    s.status |= ST_OVERFLOW;
+            } else {
+                s.open_slot = (int)slot;
+            }
+        }
+        s.cnt += (tot >> sh) & hm;
+        s.cur_ev = -1;
+        s.nev = 0;
+        w.sync();
+#pragma unroll
+        for (int k = 0; k < 8; k++) evmask[8 * lane + k] = 0u;
+        w.sync();
+    }
+
+    // lane-1's new right column and lane+1's new left column
+    BPC_FI void enc_neighbour_ns() {
+        const uint64_t up = shfl_up64(w, NS[1]), dn = shfl_down64(w, NS[0]);
+        XLN = gl > 0 ? up : 0ull;
+        XRN = gl < G::NL - 1 ? dn : 0ull;
+    }
+
+    // Compute_Context :164-172 for every row, with the neighbours' significance
+    // as each coefficient's step sees it (Share_*_Borders :342-388).
+    BPC_FI void enc_contexts() {
+        const uint64_t S0 = s.S[0], S1 = s.S[1];
+        const uint64_t Le = S0 | NS[0], Re = S1 | NS[1], XLe = XLS | XLN, XRe = XRS | XRN;
+        uint64_t x[8];
+        x[0] = XLe << 1;  // (i-1, lane-1 right)
+        x[1] = Le << 1;   // (i-1, left)
+        x[2] = Re << 1;   // (i-1, right)
+        x[3] = XLS;       // (i, lane-1 right): later in scan
+        x[4] = S1;        // (i, right): later
+        x[5] = XLS >> 1;  // (i+1, *): later
+        x[6] = S0 >> 1;
+        x[7] = S1 >> 1;
+        count8(x, cs[0][0], cs[0][1], cs[0][2], cs[0][3]);
+        x[0] = Le << 1;
+        x[1] = Re << 1;
+        x[2] = XRe << 1;
+        x[3] = Le;   // (i, left): earlier in scan
+        x[4] = XRe;  // (i, lane+1 left): earlier
+        x[5] = S0 >> 1;
+        x[6] = S1 >> 1;
+        x[7] = XRS >> 1;
+        count8(x, cs[1][0], cs[1][1], cs[1][2], cs[1][3]);
+    }
+
+    // Compute_Sign_Context :214-226 for a coefficient that became significant
+    BPC_FI int enc_sign_ctx(int i, int c) {
+        const uint64_t Le = s.S[0] | NS[0], Re = s.S[1] | NS[1];
+        // c is a runtime value here: select, never index (keeps the state in registers)
+        const uint64_t Me = c ? Re : Le, Ml = c ? s.S[1] : s.S[0], Nc = c ? s.N[1] : s.N[0];
+        const int us = i ? (int)bit64(Me, i - 1) : 0, un = i ? (int)bit64(Nc, i - 1) : 0;
+        const int bs = (int)bit64(Ml >> 1, i), bn = (int)bit64(Nc >> 1, i);
+        int ls, ln, rs, rn;
+        if (c == 0) {
+            ls = (int)bit64(XLS, i);
+            ln = (int)bit64(s.XNL, i);
+            rs = (int)bit64(s.S[1], i);
+            rn = (int)bit64(s.N[1], i);
+        } else {
+            ls = (int)bit64(Le, i);
+            ln = (int)bit64(s.N[0], i);
+            rs = (int)bit64(XRS | XRN, i);
+            rn = (int)bit64(s.XNR, i);
+        }
+        const int h = ls * (1 - 2 * ln) + rs * (1 - 2 * rn);
+        const int v = us * (1 - 2 * un) + bs * (1 - 2 * bn);
+        const int hc = h == 0 ? 0 : (h > 0 ? 1 : 2), vc = v == 0 ? 0 : (v > 0 ? 1 : 2);
+        return (int)((kSignTab >> (3 * (hc * 3 + vc))) & 7u);
+    }
+
+    // 3-pass SPP (:412-456): a non-significant coefficient is coded only if a
+    // neighbour is significant when its step comes, and coding can make it
+    // significant, so significance spreads within the pass.  A coefficient's
+    // "dynamic" neighbours are the ones earlier in scan order, so the new
+    // significance set is the least fixed point of
+    //   new = PN & (static | dyn(new)),  PN = non-significant with data bit 1,
+    // reached from new = PN & static in as many rounds as the longest chain.
+    BPC_FI void enc_spp3_propagate(bool act, bool lowp) {
+        const uint64_t S0 = s.S[0], S1 = s.S[1];
+        const uint64_t dXL = XLS | (XLS << 1) | (XLS >> 1), dXR = XRS | (XRS << 1) | (XRS >> 1);
+        const uint64_t dS0 = S0 | (S0 << 1) | (S0 >> 1), dS1 = S1 | (S1 << 1) | (S1 >> 1);
+        const uint64_t statL = dXL | (S0 << 1) | (S0 >> 1) | dS1;
+        const uint64_t statR = dS0 | (S1 << 1) | (S1 >> 1) | dXR;
+        const uint64_t cand0 = act ? ~S0 & G::ROWS : 0ull, cand1 = act ? ~S1 & G::ROWS : 0ull;
+        const uint64_t pn0 = lowp ? cand0 & B[0] : 0ull, pn1 = lowp ? cand1 & B[1] : 0ull;
+        uint64_t ns0 = pn0 & statL, ns1 = pn1 & statR, nxl = 0, nxr = 0;
+        for (;;) {
+            const uint64_t up = shfl_up64(w, ns1), dn = shfl_down64(w, ns0);
+            nxl = gl > 0 ? up : 0ull;
+            nxr = gl < G::NL - 1 ? dn : 0ull;
+            const uint64_t n0 = pn0 & (statL | ((nxl | ns0 | ns1) << 1));
+            const uint64_t n1 = pn1 & (statR | ((n0 | ns1 | nxr) << 1) | n0 | nxr);
+            const bool changed = (n0 != ns0) || (n1 != ns1);
+            ns0 = n0;
+            ns1 = n1;
+            if (!w.any(changed)) break;
+        }
+        NS[0] = ns0;
+        NS[1] = ns1;
+        XLN = nxl;
+        XRN = nxr;
+        const uint64_t dynL = (nxl | ns0 | ns1) << 1;
+        const uint64_t dynR = ((ns0 | ns1 | nxr) << 1) | ns0 | nxr;
+        K[0] = cand0 & (statL | dynL);
+        K[1] = cand1 & (statR | dynR);
+        s.C[0] |= cand0 & ~K[0];  // deferred to CP (:450-452)
+        s.C[1] |= cand1 & ~K[1];
+    }
+
+    template <int PK>
+    BPC_FI void enc_pass(int b, bool act) {
+        const int off = PK == PK_CP ? p.cp_off : 0;
+        const int sig_b = off + p.a_sig + (g + b) * 9, sign_b = off + p.a_sign + (g + b) * 4;
+        const bool lowp = b <= 27;
+#pragma unroll
+        for (int c = 0; c < 2; c++) {
+            if (PK == PK_MRP) {
+                K[c] = act ? s.R[c] : 0ull;
+                Y[c] = lowp ? (K[c] & B[c]) : ((b == 28 || b == 30) ? K[c] : 0ull);
+                NS[c] = 0ull;
+            } else if (PK == PK_CP) {
+                K[c] = act ? s.C[c] : 0ull;
+                NS[c] = lowp ? (K[c] & B[c]) : 0ull;
+                Y[c] = lowp ? NS[c] : (b == 29 ? K[c] : 0ull);
+            } else if (PASSES == 2) {
+                K[c] = act ? (~s.S[c] & G::ROWS) : 0ull;
+                NS[c] = lowp ? (K[c] & B[c]) : 0ull;
+                Y[c] = NS[c];
+            }
+        }
+        if (PK == PK_SPP && PASSES == 3) {
+            enc_spp3_propagate(act, lowp);
+            Y[0] = NS[0];
+            Y[1] = NS[1];
+        } else if (PK != PK_MRP) {
+            enc_neighbour_ns();
+        }
+        if (PK != PK_MRP) enc_contexts();
+        const uint32_t Pref = PK == PK_MRP && act ? (uint32_t)tab[g + b] : 0u;
+        // one lane's coded symbols in scan order: 16 rows at a time, the two
+        // columns interleaved so that position t = 2*row + column
+#pragma unroll 1
+        for (int q = 0; q < CBS / 16; q++) {
+            uint32_t kq = zip16(K[0], K[1], q);
+            if (!kq) continue;
+            const uint32_t yq = zip16(Y[0], Y[1], q);
+            uint32_t nq = 0, c0 = 0, c1 = 0, c2 = 0, c3 = 0;
+            if (PK != PK_MRP) {
+                nq = zip16(NS[0], NS[1], q);
+                c0 = zip16(cs[0][0], cs[1][0], q);
+                c1 = zip16(cs[0][1], cs[1][1], q);
+                c2 = zip16(cs[0][2], cs[1][2], q);
+                c3 = zip16(cs[0][3], cs[1][3], q);
+            }
+            do {
+                const int t = ctz64(kq);
+                kq &= kq - 1;
+                const int key = (32 * q + t) * 2;  // (row, column, phase) in the pass
+                uint32_t P;
+                if (PK == PK_MRP) {
+                    P = Pref;
+                } else {
+                    const uint32_t ctx = ((c0 >> t) & 1u) | (((c1 >> t) & 1u) << 1) | (((c2 >> t) & 1u) << 2) |
+                                         (((c3 >> t) & 1u) << 3);
+                    P = tab[sig_b + (int)ctx];
+                }
+                enc_symbol((yq >> t) & 1u, P, key);
+                if (PK != PK_MRP && ((nq >> t) & 1u)) {
+                    const int i = 16 * q + (t >> 1), c = t & 1;
+                    const int sctx = enc_sign_ctx(i, c);
+                    const uint64_t Nc = c ? s.N[1] : s.N[0];
+                    enc_symbol(bit64(Nc, i) ^ (uint32_t)(sctx & 1), tab[sign_b + (sctx >> 1)], key + 1);
+                }
+            } while (kq);
+        }
+        enc_rank();
+        if (PK == PK_MRP) {
+            if (act) {
+                s.R[0] = s.S[0];
+                s.R[1] = s.S[1];
+            }
+        } else {
+            s.S[0] |= NS[0];
+            s.S[1] |= NS[1];
+            XLS |= XLN;
+            XRS |= XRN;
+            if (PK == PK_CP) {
+                s.R[0] |= NS[0];
+                s.R[1] |= NS[1];
+                s.C[0] &= ~K[0];
+                s.C[1] &= ~K[1];
+            }
+        }
+    }
+
     // ------------------------------------------------------ codeblock driver
     BPC_FI void run(int cb_first) {
         const int grp = lane / G::NL;
@@ -471,6 +794,14 @@ struct Coder {
         s.cnt = 0u;
         s.has_resv = 0;
         s.status = 0;
+        s.open_slot = -1;
+        s.cur_ev = -1;
+        s.nev = 0;
+        XLS = XRS = XLN = XRN = 0ull;
+        if (ENC) {
+            for (int k = 0; k < 8; k++) evmask[8 * lane + k] = 0u;
+            w.sync();
+        }
         const size_t cap = (size_t)G::CAP;
         const int32_t *src = p.in + (size_t)y0 * (size_t)p.X + (size_t)x;
         msb = -1;
@@ -548,18 +879,26 @@ struct Coder {
             const bool full = PASSES == 2 ? b <= msb : b < msb;
             const bool first_cp = PASSES == 3 && b == msb;
             plane_begin(b);
-            if (w.any(full)) {
-                ctx_pass<PK_SPP>(b, full);
-                mrp_pass(b, full);
+            if (ENC) {
+                if (w.any(full)) {
+                    enc_pass<PK_SPP>(b, full);
+                    enc_pass<PK_MRP>(b, full);
+                }
+                if (PASSES == 3 && w.any(full || first_cp)) enc_pass<PK_CP>(b, full || first_cp);
+            } else {
+                if (w.any(full)) {
+                    ctx_pass<PK_SPP>(b, full);
+                    mrp_pass(b, full);
+                }
+                if (PASSES == 3 && w.any(full || first_cp)) ctx_pass<PK_CP>(b, full || first_cp);
             }
-            if (PASSES == 3 && w.any(full || first_cp)) ctx_pass<PK_CP>(b, full || first_cp);
             if (b <= msb) plane_end(b);
         }
         if (ENC) {
             if (ok) {
-                if (s.has_resv) {  // flush :1020
-                    if (s.resv < (uint32_t)G::CAP)
-                        slot_out[s.resv] = (int32_t)s.lower;
+                if (s.has_resv && s.size != 0) {  // flush :1020 (a finished codeword is already stored)
+                    if (s.open_slot < G::CAP)
+                        slot_out[s.open_slot] = (int32_t)s.lower;
                     else
                         s.status |= ST_OVERFLOW;
                 }
@@ -578,7 +917,7 @@ struct Coder {
 #pragma unroll
                 for (int k = 0; k < 32; k++) a[k] = (k < 28 && k <= top) ? planes[k < 28 ? k : 0][c * 2 + h] : 0u;
                 transpose32(a);
-                const uint64_t neg = s.N[c] >> (32 * h);
+                const uint64_t neg = (c ? s.N[1] : s.N[0]) >> (32 * h);
 #pragma unroll
                 for (int r = 0; r < 32; r++) {
                     const int32_t m = (int32_t)a[r];

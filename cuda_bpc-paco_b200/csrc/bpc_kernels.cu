@@ -4,8 +4,8 @@
 // kWarps warps stages the LUT once into shared memory as bytes and then walks
 // codeblocks grid-stride, so the same kernel serves the plain one-image launch
 // (grid = ceil(ncb / kWarps)) and a persistent launch (grid = k * 148).
-// kMinCtas CTAs per SM (28 warps) keep every codeblock of a 4096x4096 image
-// resident in one wave.
+// The decoder's kMinCtasDec CTAs per SM (28 warps) keep every codeblock of a
+// 4096x4096 image resident in one wave.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -21,6 +21,8 @@ struct GpuWarp {
     __device__ __forceinline__ uint32_t shfl_xor(uint32_t v, int o) { return __shfl_xor_sync(0xffffffffu, v, o); }
     __device__ __forceinline__ uint32_t shfl_up(uint32_t v, int d) { return __shfl_up_sync(0xffffffffu, v, d); }
     __device__ __forceinline__ uint32_t shfl_down(uint32_t v, int d) { return __shfl_down_sync(0xffffffffu, v, d); }
+    __device__ __forceinline__ uint32_t shfl_idx(uint32_t v, int l) { return __shfl_sync(0xffffffffu, v, l); }
+    __device__ __forceinline__ void smem_or(uint32_t *p, uint32_t v) { atomicOr(p, v); }
     __device__ __forceinline__ void sync() { __syncwarp(); }
     __device__ __forceinline__ void syncmask(uint32_t m) { __syncwarp(m); }
     __device__ __forceinline__ void load2(const int32_t *p, int32_t &a, int32_t &b) {
@@ -44,7 +46,7 @@ struct GpuWarp {
 };
 
 template <int PASSES, int CBS, bool ENC>
-__global__ void __launch_bounds__(kWarps * 32, kMinCtas) k_bpc(Params p) {
+__global__ void __launch_bounds__(kWarps * 32, ENC ? kMinCtasEnc : kMinCtasDec) k_bpc(Params p) {
     using G = Geo<CBS>;
     extern __shared__ __align__(16) unsigned char smem[];
     uint8_t *tab = smem;
@@ -60,11 +62,15 @@ __global__ void __launch_bounds__(kWarps * 32, kMinCtas) k_bpc(Params p) {
     if (bad && p.status) atomicOr(p.status, ST_LUT_RANGE);
     __syncthreads();
     const int warp = (int)(threadIdx.x >> 5);
-    uint32_t *ring = reinterpret_cast<uint32_t *>(smem + p.tab_n) + warp * G::RING_WORDS;
+    // per warp: the decoder's codeword ring, or the encoder's event ranking words
+    uint32_t *ring = reinterpret_cast<uint32_t *>(smem + p.tab_n) + warp * (ENC ? 512 : G::RING_WORDS);
     GpuWarp w;
+    uint32_t planes[28][4];  // per-thread bitplanes (local memory, L1-resident)
+    uint8_t ev_key[ENC ? 256 : 1];
+    uint32_t ev_val[ENC ? 256 : 1];
     const int stride = (int)gridDim.x * kWarps * G::NG;
     for (int base = ((int)blockIdx.x * kWarps + warp) * G::NG; base < p.ncb; base += stride) {
-        Coder<PASSES, CBS, ENC, GpuWarp> cd(w, p, ring, tab);
+        Coder<PASSES, CBS, ENC, GpuWarp> cd(w, p, ring, tab, planes, ev_key, ev_val);
         cd.run(base);
     }
 }
@@ -72,7 +78,7 @@ __global__ void __launch_bounds__(kWarps * 32, kMinCtas) k_bpc(Params p) {
 template <int PASSES, int CBS, bool ENC>
 static size_t smem_bytes(const Params &p) {
     using G = Geo<CBS>;
-    return (size_t)p.tab_n + (size_t)kWarps * 4u * (size_t)(ENC ? 0 : G::RING_WORDS);
+    return (size_t)p.tab_n + (size_t)kWarps * 4u * (size_t)(ENC ? 512 : G::RING_WORDS);
 }
 
 template <int PASSES, int CBS, bool ENC>

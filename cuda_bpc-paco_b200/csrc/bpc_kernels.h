@@ -5,10 +5,19 @@
 
 #include "bpc_core.cuh"
 
+#ifndef ENC_MIN_CTAS
+#define ENC_MIN_CTAS 4
+#endif
+
 namespace bpc {
 
-constexpr int kWarps = 4;    // warps (codeblocks) per CTA
-constexpr int kMinCtas = 7;  // CTAs per SM the register budget is sized for
+constexpr int kWarps = 4;  // warps (codeblocks) per CTA
+// CTAs per SM the register budget is sized for: the decoder steps its lanes
+// together and needs many warps to hide latency (7 x 4 warps, <= 72
+// registers); the encoder runs each lane's coder on its own and needs the
+// registers more than the warps.
+constexpr int kMinCtasDec = 7;
+constexpr int kMinCtasEnc = ENC_MIN_CTAS;
 
 // Launch the encoder (enc) or decoder over p.ncb codeblocks.  grid <= 0 picks
 // one CTA per kWarps codeblocks; a positive grid runs persistent CTAs that
