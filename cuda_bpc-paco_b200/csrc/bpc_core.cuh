@@ -142,6 +142,31 @@ BPC_FI void transpose32(uint32_t a[32]) {
 
 BPC_FI uint32_t bit64(uint64_t m, int i) { return (uint32_t)(m >> i) & 1u; }
 
+BPC_FI uint32_t funnel_r(uint32_t lo, uint32_t hi, int n) {
+#if defined(__CUDA_ARCH__)
+    return __funnelshift_r(lo, hi, n);
+#else
+    return (uint32_t)((((uint64_t)hi << 32) | lo) >> (n & 31));
+#endif
+}
+
+// Row access inside one 32-row half H of a 64-bit column mask (row i = 32H + j):
+// 32-bit shifts only.  win3h gives rows i-1, i, i+1 (0 outside the block).
+template <int H>
+BPC_FI uint32_t win3h(uint64_t m, int j) {
+    const uint32_t lo = (uint32_t)m, hi = (uint32_t)(m >> 32);
+    const uint32_t t = H == 0 ? (j ? funnel_r(lo, hi, j - 1) : (lo << 1)) : (j ? (hi >> (j - 1)) : funnel_r(lo, hi, 31));
+    return t & 7u;
+}
+template <int H>
+BPC_FI uint32_t bith(uint64_t m, int j) {
+    return ((H ? (uint32_t)(m >> 32) : (uint32_t)m) >> j) & 1u;
+}
+template <int H>
+BPC_FI uint64_t maskh(uint32_t bit, int j) {
+    return (uint64_t)(bit << j) << (32 * H);
+}
+
 // Interleave the low 16 bits of a (even positions) and b (odd positions):
 // row j of the left column -> bit 2j, of the right column -> bit 2j+1, which
 // is the scan order of one lane's two columns.
@@ -228,6 +253,8 @@ struct Coder {
     // masks, neighbour columns' significance at pass start and new in pass
     uint64_t K[2], Y[2], NS[2], XLS, XRS, XLN, XRN;
     uint64_t cs[2][4];  // context bit slices per column
+    uint64_t si[2][2];  // sign-context LUT index bit slices per column
+    uint64_t sg[2];     // sign symbol per column (own sign ^ predicted sign)
     uint32_t *evmask;   // per warp, 256 keys: lanes with a reservation event
     uint32_t *pfx;      // per warp, 256 keys: events before the key (ranking)
     uint8_t *ev_key;    // this lane's events of the pass: key, finished codeword
@@ -251,50 +278,25 @@ struct Coder {
     }
 
     // ---------------------------------------------------------------- AC
-    // Arithmetic_encoder :261-295
-    BPC_FI void ac_enc(bool act, uint32_t sym, uint32_t P) {
-        const bool need = act && s.size == 0;
-        const uint32_t bal = w.ballot(need) & gmask;
-        if (need) {
-            s.resv = 1u + s.cnt + (uint32_t)popc32(bal & ltmask);
-            s.has_resv = 1;
-            s.lower = 0;
-            s.size = 0xFFFFu;
-        }
-        s.cnt += (uint32_t)popc32(bal);
-        if (act) {
-            const uint32_t t = ((s.size * P) >> 7) + sym;
-            if (sym) {
-                s.size -= t;
-                s.lower += t;
-            } else {
-                s.size = t;
-            }
-            if (s.size == 0) {
-                if (s.resv < (uint32_t)G::CAP)
-                    slot_out[s.resv] = (int32_t)s.lower;
-                else
-                    s.status |= ST_OVERFLOW;
-            }
-        }
-    }
-
     // Arithmetic_decoder :297-339; the codeword is read when it is reserved
     BPC_FI uint32_t ac_dec(bool act, uint32_t P) {
         const bool need = act && s.size == 0;
-        const uint32_t bal = w.ballot(need) & gmask;
-        if (need) {
-            const uint32_t idx = 1u + s.cnt + (uint32_t)popc32(bal & ltmask);
-            if (idx < (uint32_t)G::CAP) {
-                s.cw = ring[idx & (G::RING - 1)];
-            } else {
-                s.cw = 0xFFFFFFFFu;
-                s.status |= ST_OVERFLOW;
+        const uint32_t ball = w.ballot(need);
+        if (ball) {  // warp-uniform
+            const uint32_t bal = ball & gmask;
+            if (need) {
+                const uint32_t idx = 1u + s.cnt + (uint32_t)popc32(bal & ltmask);
+                if (idx < (uint32_t)G::CAP) {
+                    s.cw = ring[idx & (G::RING - 1)];
+                } else {
+                    s.cw = 0xFFFFFFFFu;
+                    s.status |= ST_OVERFLOW;
+                }
+                s.lower = 0;
+                s.size = 0xFFFFu;
             }
-            s.lower = 0;
-            s.size = 0xFFFFu;
+            s.cnt += (uint32_t)popc32(bal);
         }
-        s.cnt += (uint32_t)popc32(bal);
         uint32_t sym = 0;
         if (act) {
             const uint32_t t = ((s.size * P) >> 7) + 1u;
@@ -347,18 +349,6 @@ struct Coder {
     // MSB = 32, where 3 << 32 is 0 and the mask stays 0 until plane 0.
     BPC_FI bool keep_bit(int b) const { return msb != 32 || b == 0; }
 
-    // Data bit the encoder codes at plane b: magnitude bit b for b <= 27; above
-    // that the reference reads its flag bits (b+1 = 29 R, 30 C, 31 sigma, 32+
-    // nothing), which for the coefficients each pass visits gives these
-    // constants.  Planes >= 28 are only visited by all-zero codeblocks (MSB 32).
-    template <int PK>
-    BPC_FI uint32_t data_bit(int i, int c, int b) {
-        if (b <= 27) return (uint32_t)(B[c] >> i) & 1u;
-        if (PK == PK_CP) return b == 29 ? 1u : 0u;
-        if (PK == PK_MRP) return (b == 28 || b == 30) ? 1u : 0u;
-        return 0u;
-    }
-
     // plane registers: encoder loads the magnitude bits, decoder clears
     BPC_FI void plane_begin(int b) {
         if (ENC) {
@@ -383,114 +373,136 @@ struct Coder {
         }
     }
 
-    // ------------------------------------------------------- context steps
-    template <int PK, int c>
-    BPC_FI void ctx_step(int i, int b, bool act) {
-        const uint64_t bit = 1ull << i;
-        const bool cand = act && (PK == PK_SPP ? !((s.S[c] >> i) & 1) : ((s.C[c] >> i) & 1));
+    // ------------------------------------------ decoder: lockstep over steps
+    // The decoder cannot run ahead per lane: a context depends on what the
+    // neighbour lanes decoded one step earlier, and a reservation needs the
+    // number of reservations before it.  So the warp walks the steps that
+    // have a candidate in some lane, all lanes together, and the rows are
+    // visited per 32-row half so that every row access is a 32-bit shift.
+    // One step (row 32H + j, column c).  c is a run-time value so that the
+    // decoder has one step body per pass kind and half: warps in different
+    // passes share the instruction cache.
+    template <int PK, int H>
+    BPC_FI void dec_ctx_step(int j, int c, int b, bool act) {
+        const uint64_t S0 = s.S[0], S1 = s.S[1], Sc = c ? S1 : S0;
+        const bool cand = act && (PK == PK_SPP ? !bith<H>(Sc, j) : bith<H>(c ? s.C[1] : s.C[0], j));
         if (!w.any(cand)) return;
-        if (!ENC) ring_ensure();
-        const uint64_t Lm = c ? s.S[0] : s.XL, Mm = s.S[c], Rm = c ? s.XR : s.S[1];
-        const uint32_t wl = win3(Lm, i), wm = win3(Mm, i), wr = win3(Rm, i);
+        ring_ensure();
+        const uint64_t Lm = c ? S0 : s.XL, Rm = c ? s.XR : S1;
+        const uint32_t wl = win3h<H>(Lm, j), wm = win3h<H>(Sc, j), wr = win3h<H>(Rm, j);
         const uint32_t nbh = wl | ((wm & 5u) << 3) | (wr << 6);
+        const uint64_t bit = maskh<H>(1u, j), bit0 = c ? 0ull : bit, bit1 = c ? bit : 0ull;
         bool coded = cand;
         if (PK == PK_SPP && PASSES == 3) {
-            if (cand && nbh == 0) {
-                s.C[c] |= bit;  // SPP defers to CP (:450-452)
+            if (cand && nbh == 0) {  // SPP defers to CP (:450-452)
+                s.C[0] |= bit0;
+                s.C[1] |= bit1;
                 coded = false;
             }
         }
-        const int ctx = popc32(nbh);
-        const uint32_t P = coded ? tab[sig_base + ctx] : 0u;
-        uint32_t sym;
-        if (ENC) {
-            sym = coded ? data_bit<PK>(i, c, b) : 0u;
-            ac_enc(coded, sym, P);
-        } else {
-            sym = ac_dec(coded, P);
+        const uint32_t P = coded ? tab[sig_base + popc32(nbh)] : 0u;
+        const uint32_t sym = ac_dec(coded, P);
+        if (PK == PK_CP && coded) {
+            s.C[0] &= ~bit0;
+            s.C[1] &= ~bit1;
         }
-        if (PK == PK_CP && coded) s.C[c] &= ~bit;
         const bool ns = coded && sym && b <= 27;
         if (ns) {
-            s.S[c] |= bit;
-            if (PK == PK_CP) s.R[c] |= bit;
-            if (!ENC) B[c] |= bit;
+            s.S[0] |= bit0;
+            s.S[1] |= bit1;
+            if (PK == PK_CP) {
+                s.R[0] |= bit0;
+                s.R[1] |= bit1;
+            }
+            B[0] |= bit0;
+            B[1] |= bit1;
         }
         if (!w.any(ns)) return;
-        // sign call (Compute_Sign_Context :214-226 over u, l, r, b)
-        const uint64_t LN = c ? s.N[0] : s.XNL, MN = s.N[c], RN = c ? s.XNR : s.N[1];
-        const int ls = (wl >> 1) & 1, rs = (wr >> 1) & 1, us = wm & 1, bs = (wm >> 2) & 1;
-        const int ln = (int)((LN >> i) & 1), rn = (int)((RN >> i) & 1);
-        const uint32_t wmn = win3(MN, i);
-        const int un = wmn & 1, bn = (wmn >> 2) & 1;
-        const int h = ls * (1 - 2 * ln) + rs * (1 - 2 * rn);
-        const int v = us * (1 - 2 * un) + bs * (1 - 2 * bn);
-        const int hc = h == 0 ? 0 : (h > 0 ? 1 : 2), vc = v == 0 ? 0 : (v > 0 ? 1 : 2);
-        const int sctx = (int)((kSignTab >> (3 * (hc * 3 + vc))) & 7u);
-        const uint32_t P2 = ns ? tab[sign_base + (sctx >> 1)] : 0u;
-        uint32_t neg;
-        if (ENC) {
-            neg = (uint32_t)((s.N[c] >> i) & 1);
-            ac_enc(ns, neg ^ (uint32_t)(sctx & 1), P2);
-        } else {
-            neg = ac_dec(ns, P2) ^ (uint32_t)(sctx & 1);
-            if (ns && neg) s.N[c] |= bit;
+        // sign call (Compute_Sign_Context :178-226 over u, l, r, b), the table
+        // as boolean functions of the sign-sum classes (see enc_sign_slices)
+        const uint64_t LN = c ? s.N[0] : s.XNL, MN = c ? s.N[1] : s.N[0], RN = c ? s.XNR : s.N[1];
+        const uint32_t sl = (wl >> 1) & 1u, sr = (wr >> 1) & 1u, su = wm & 1u, sb = (wm >> 2) & 1u;
+        const uint32_t nl = bith<H>(LN, j), nr = bith<H>(RN, j), wmn = win3h<H>(MN, j);
+        const uint32_t nu = wmn & 1u, nb = (wmn >> 2) & 1u;
+        const uint32_t pl = sl & ~nl, ml = sl & nl, pr = sr & ~nr, mr = sr & nr;
+        const uint32_t pu = su & ~nu, mu = su & nu, pb = sb & ~nb, mb = sb & nb;
+        const uint32_t hp = (pl & ~mr) | (pr & ~ml), hn = (ml & ~pr) | (mr & ~pl);
+        const uint32_t vp = (pu & ~mb) | (pb & ~mu), vn = (mu & ~pb) | (mb & ~pu);
+        const uint32_t h0 = ~(hp | hn) & 1u, v0 = ~(vp | vn) & 1u;
+        const uint32_t sidx = ((h0 & ~v0) | (hp & vp) | (hn & vn)) | (((hp & ~vn) | (hn & ~vp)) << 1);
+        const uint32_t pred = (h0 & vn) | hn;
+        const uint32_t P2 = ns ? tab[sign_base + (int)(sidx & 3u)] : 0u;
+        const uint32_t neg = (ac_dec(ns, P2) ^ pred) & 1u;
+        if (ns && neg) {
+            s.N[0] |= bit0;
+            s.N[1] |= bit1;
         }
-        // neighbour columns: lane l's column c at row i changed
-        const uint32_t bsig = w.ballot(ns);
-        const uint32_t bneg = ENC ? 0u : w.ballot(ns && neg);
+        // neighbour columns: lane l's column c at row i changed; lane l-1
+        // (column 0) or lane l+1 (column 1) takes it over with one shuffle
+        const uint32_t mine = ns ? (1u | (neg << 1)) : 0u;
+        const int src = c ? lane - 1 : lane + 1;
+        const uint32_t got = w.shfl_idx(mine, src & 31);
         if (c == 0) {
             if (gl < G::NL - 1) {
-                s.XR |= (uint64_t)((bsig >> (lane + 1)) & 1u) << i;
-                if (!ENC) s.XNR |= (uint64_t)((bneg >> (lane + 1)) & 1u) << i;
+                s.XR |= maskh<H>(got & 1u, j);
+                s.XNR |= maskh<H>((got >> 1) & 1u, j);
             }
         } else {
             if (gl > 0) {
-                s.XL |= (uint64_t)((bsig >> (lane - 1)) & 1u) << i;
-                if (!ENC) s.XNL |= (uint64_t)((bneg >> (lane - 1)) & 1u) << i;
+                s.XL |= maskh<H>(got & 1u, j);
+                s.XNL |= maskh<H>((got >> 1) & 1u, j);
             }
         }
     }
 
+    template <int PK, int H>
+    BPC_FI void dec_ctx_half(uint32_t u, int b, bool act) {
+        while (u) {
+            const int j = ctz64(u);
+            u &= u - 1;
+#pragma unroll 1
+            for (int c = 0; c < 2; c++) dec_ctx_step<PK, H>(j, c, b, act);
+        }
+    }
+
     template <int PK>
-    BPC_FI void ctx_pass(int b, bool act) {
+    BPC_FI void dec_ctx_pass(int b, bool act) {
         const int off = PK == PK_CP ? p.cp_off : 0;
         sig_base = off + p.a_sig + (g + b) * 9;
         sign_base = off + p.a_sign + (g + b) * 4;
         const uint64_t c0 = act ? (PK == PK_SPP ? ~s.S[0] : s.C[0]) : 0ull;
         const uint64_t c1 = act ? (PK == PK_SPP ? ~s.S[1] : s.C[1]) : 0ull;
-        uint64_t U = warp_or64(w, (c0 | c1) & G::ROWS);
-        while (U) {
-            const int i = ctz64(U);
-            U &= U - 1;
-            ctx_step<PK, 0>(i, b, act);
-            ctx_step<PK, 1>(i, b, act);
+        const uint64_t U = warp_or64(w, (c0 | c1) & G::ROWS);
+        dec_ctx_half<PK, 0>((uint32_t)U, b, act);
+        if (CBS == 64) dec_ctx_half<PK, 1>((uint32_t)(U >> 32), b, act);
+    }
+
+    // MRP_Decoder :608-629
+    template <int H>
+    BPC_FI void dec_mrp_half(uint32_t u, int b, bool act, uint32_t P) {
+        while (u) {
+            const int j = ctz64(u);
+            u &= u - 1;
+#pragma unroll 1
+            for (int c = 0; c < 2; c++) {
+                const bool cand = act && bith<H>(c ? s.R[1] : s.R[0], j);
+                if (!w.any(cand)) continue;
+                ring_ensure();
+                const uint32_t sym = ac_dec(cand, P);
+                if (cand && sym && b <= 27) {
+                    const uint64_t bit = maskh<H>(1u, j);
+                    B[0] |= c ? 0ull : bit;
+                    B[1] |= c ? bit : 0ull;
+                }
+            }
         }
     }
 
-    // MRP_Encoder/Decoder :593-629
-    template <int c>
-    BPC_FI void mrp_step(int i, int b, bool act, uint32_t P) {
-        const bool cand = act && ((s.R[c] >> i) & 1);
-        if (!w.any(cand)) return;
-        if (ENC) {
-            ac_enc(cand, cand ? data_bit<PK_MRP>(i, c, b) : 0u, P);
-        } else {
-            ring_ensure();
-            const uint32_t sym = ac_dec(cand, P);
-            if (cand && sym && b <= 27) B[c] |= 1ull << i;
-        }
-    }
-
-    BPC_FI void mrp_pass(int b, bool act) {
+    BPC_FI void dec_mrp_pass(int b, bool act) {
         const uint32_t P = act ? tab[g + b] : 0u;
-        uint64_t U = warp_or64(w, act ? ((s.R[0] | s.R[1]) & G::ROWS) : 0ull);
-        while (U) {
-            const int i = ctz64(U);
-            U &= U - 1;
-            mrp_step<0>(i, b, act, P);
-            mrp_step<1>(i, b, act, P);
-        }
+        const uint64_t U = warp_or64(w, act ? ((s.R[0] | s.R[1]) & G::ROWS) : 0ull);
+        dec_mrp_half<0>((uint32_t)U, b, act, P);
+        if (CBS == 64) dec_mrp_half<1>((uint32_t)(U >> 32), b, act, P);
         if (act) {
             s.R[0] = s.S[0];
             s.R[1] = s.S[1];
@@ -508,7 +520,36 @@ struct Coder {
     // warp ranks all events by (key, lane) -- the reference's lockstep order --
     // and the codewords go to their slots.
 
-    // Arithmetic_encoder :261-295 for this lane; reservation -> event
+    // Arithmetic_encoder :261-295 for this lane; reservation -> event.  `on`
+    // predicates the call so that the optional sign call needs no branch.
+    BPC_FI void enc_symbol_if(bool on, uint32_t sym, uint32_t P, int key) {
+        if (on && s.size == 0) {
+            ev_key[s.nev] = (uint8_t)key;
+            ev_val[s.nev] = 0u;
+            s.cur_ev = s.nev;
+            s.nev++;
+            w.smem_or(&evmask[key], 1u << lane);
+            s.has_resv = 1;
+            s.lower = 0;
+            s.size = 0xFFFFu;
+        }
+        const uint32_t t = ((s.size * P) >> 7) + sym;
+        const uint32_t nsize = sym ? s.size - t : t;
+        const uint32_t nlow = sym ? s.lower + t : s.lower;
+        if (on) {
+            s.size = nsize;
+            s.lower = nlow;
+        }
+        if (on && nsize == 0) {
+            if (s.cur_ev >= 0)
+                ev_val[s.cur_ev] = nlow;
+            else if (s.open_slot < G::CAP)
+                slot_out[s.open_slot] = (int32_t)nlow;
+            else
+                s.status |= ST_OVERFLOW;
+        }
+    }
+
     BPC_FI void enc_symbol(uint32_t sym, uint32_t P, int key) {
         if (s.size == 0) {
             ev_key[s.nev] = (uint8_t)key;
@@ -619,6 +660,39 @@ struct Coder {
         count8(x, cs[1][0], cs[1][1], cs[1][2], cs[1][3]);
     }
 
+    // Compute_Sign_Context :178-226 for every row at once.  With pos/neg the
+    // significant-positive / significant-negative neighbours, the sums
+    // h = sgn(l) + sgn(r) and v = sgn(u) + sgn(b) reduce to the classes
+    // h > 0 = (pl & ~nr) | (pr & ~nl), h < 0 = (nl & ~pr) | (nr & ~pl), and the
+    // table of :184-208 to three boolean functions of the classes: the LUT
+    // index (ctx >> 1) bits and the predicted-sign bit (ctx & 1).
+    BPC_FI void enc_sign_slices() {
+        const uint64_t Le = s.S[0] | NS[0], Re = s.S[1] | NS[1], XRe = XRS | XRN;
+#pragma unroll
+        for (int c = 0; c < 2; c++) {
+            uint64_t sl, nl, sr, nr, su, nu, sb, nb;
+            if (c == 0) {
+                sl = XLS; nl = s.XNL;                   // (i, lane-1 right): later
+                sr = s.S[1]; nr = s.N[1];               // (i, right): later
+                su = Le << 1; nu = s.N[0] << 1;         // (i-1, left): earlier
+                sb = s.S[0] >> 1; nb = s.N[0] >> 1;     // (i+1, left): later
+            } else {
+                sl = Le; nl = s.N[0];                   // (i, left): earlier
+                sr = XRe; nr = s.XNR;                   // (i, lane+1 left): earlier
+                su = Re << 1; nu = s.N[1] << 1;
+                sb = s.S[1] >> 1; nb = s.N[1] >> 1;
+            }
+            const uint64_t pl = sl & ~nl, ml = sl & nl, pr = sr & ~nr, mr = sr & nr;
+            const uint64_t pu = su & ~nu, mu = su & nu, pb = sb & ~nb, mb = sb & nb;
+            const uint64_t hp = (pl & ~mr) | (pr & ~ml), hn = (ml & ~pr) | (mr & ~pl);
+            const uint64_t vp = (pu & ~mb) | (pb & ~mu), vn = (mu & ~pb) | (mb & ~pu);
+            const uint64_t h0 = ~(hp | hn), v0 = ~(vp | vn);
+            si[c][0] = (h0 & ~v0) | (hp & vp) | (hn & vn);
+            si[c][1] = (hp & ~vn) | (hn & ~vp);
+            sg[c] = s.N[c] ^ ((h0 & vn) | hn);
+        }
+    }
+
     // Compute_Sign_Context :214-226 for a coefficient that became significant
     BPC_FI int enc_sign_ctx(int i, int c) {
         const uint64_t Le = s.S[0] | NS[0], Re = s.S[1] | NS[1];
@@ -687,6 +761,12 @@ struct Coder {
     BPC_FI void enc_pass(int b, bool act) {
         const int off = PK == PK_CP ? p.cp_off : 0;
         const int sig_b = off + p.a_sig + (g + b) * 9, sign_b = off + p.a_sign + (g + b) * 4;
+        // The data bit coded at plane b is magnitude bit b for b <= 27; above
+        // that the reference reads its flag bits (b+1 = 29 refinement, 30 CP,
+        // 31 significance, >= 32 nothing), which for the coefficients each pass
+        // visits are constants: MRP reads 1 at b = 28 and 30, CP reads 1 at
+        // b = 29 (the CP flag itself) without the coefficient becoming
+        // significant (:523-530).  Planes >= 28 only occur for MSB 32.
         const bool lowp = b <= 27;
 #pragma unroll
         for (int c = 0; c < 2; c++) {
@@ -711,7 +791,10 @@ struct Coder {
         } else if (PK != PK_MRP) {
             enc_neighbour_ns();
         }
-        if (PK != PK_MRP) enc_contexts();
+        if (PK != PK_MRP) {
+            enc_contexts();
+            enc_sign_slices();
+        }
         const uint32_t Pref = PK == PK_MRP && act ? (uint32_t)tab[g + b] : 0u;
         // one lane's coded symbols in scan order: 16 rows at a time, the two
         // columns interleaved so that position t = 2*row + column
@@ -720,32 +803,30 @@ struct Coder {
             uint32_t kq = zip16(K[0], K[1], q);
             if (!kq) continue;
             const uint32_t yq = zip16(Y[0], Y[1], q);
-            uint32_t nq = 0, c0 = 0, c1 = 0, c2 = 0, c3 = 0;
+            uint32_t nq = 0, c0 = 0, c1 = 0, c2 = 0, c3 = 0, s0 = 0, s1 = 0, gq = 0;
             if (PK != PK_MRP) {
                 nq = zip16(NS[0], NS[1], q);
                 c0 = zip16(cs[0][0], cs[1][0], q);
                 c1 = zip16(cs[0][1], cs[1][1], q);
                 c2 = zip16(cs[0][2], cs[1][2], q);
                 c3 = zip16(cs[0][3], cs[1][3], q);
+                s0 = zip16(si[0][0], si[1][0], q);
+                s1 = zip16(si[0][1], si[1][1], q);
+                gq = zip16(sg[0], sg[1], q);
             }
             do {
                 const int t = ctz64(kq);
                 kq &= kq - 1;
                 const int key = (32 * q + t) * 2;  // (row, column, phase) in the pass
-                uint32_t P;
                 if (PK == PK_MRP) {
-                    P = Pref;
+                    enc_symbol_if(true, (yq >> t) & 1u, Pref, key);
                 } else {
                     const uint32_t ctx = ((c0 >> t) & 1u) | (((c1 >> t) & 1u) << 1) | (((c2 >> t) & 1u) << 2) |
                                          (((c3 >> t) & 1u) << 3);
-                    P = tab[sig_b + (int)ctx];
-                }
-                enc_symbol((yq >> t) & 1u, P, key);
-                if (PK != PK_MRP && ((nq >> t) & 1u)) {
-                    const int i = 16 * q + (t >> 1), c = t & 1;
-                    const int sctx = enc_sign_ctx(i, c);
-                    const uint64_t Nc = c ? s.N[1] : s.N[0];
-                    enc_symbol(bit64(Nc, i) ^ (uint32_t)(sctx & 1), tab[sign_b + (sctx >> 1)], key + 1);
+                    enc_symbol_if(true, (yq >> t) & 1u, tab[sig_b + (int)ctx], key);
+                    // the sign call of a coefficient that became significant
+                    const uint32_t sidx = ((s0 >> t) & 1u) | (((s1 >> t) & 1u) << 1);
+                    enc_symbol_if(((nq >> t) & 1u) != 0u, (gq >> t) & 1u, tab[sign_b + (int)sidx], key + 1);
                 }
             } while (kq);
         }
@@ -887,10 +968,10 @@ struct Coder {
                 if (PASSES == 3 && w.any(full || first_cp)) enc_pass<PK_CP>(b, full || first_cp);
             } else {
                 if (w.any(full)) {
-                    ctx_pass<PK_SPP>(b, full);
-                    mrp_pass(b, full);
+                    dec_ctx_pass<PK_SPP>(b, full);
+                    dec_mrp_pass(b, full);
                 }
-                if (PASSES == 3 && w.any(full || first_cp)) ctx_pass<PK_CP>(b, full || first_cp);
+                if (PASSES == 3 && w.any(full || first_cp)) dec_ctx_pass<PK_CP>(b, full || first_cp);
             }
             if (b <= msb) plane_end(b);
         }
