@@ -41,6 +41,9 @@ CONFIGS = {
     "cfg5": dict(side=16384, levels=5, passes=3, cb=64, amp=80.0, nrect=400),
 }
 METRIC = "encode/decode Gcoeff/s (bit-exact)"
+# DRAM read + write bytes of one launch of the dominant kernel (the decoder),
+# from the ncu capture summarised in profiles/k_bpc_cfg2_full.md.
+NCU_TRAFFIC = {"cfg2": 14.621440e6 + 19.690496e6}
 
 
 def workload_name(c):
@@ -71,7 +74,7 @@ class ClockSampler:
              "clocks_event_reasons.sw_power_cap")
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
-                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
@@ -147,7 +150,14 @@ def run_reference(args, c):
     lut_np = oracle.load_luts(os.path.join(LUT_DIR, f"{c['passes']}_coding_pass"), c["passes"], c["levels"])
     threads = os.cpu_count() or 1
     ncb = (img.shape[0] // c["cb"]) * (img.shape[1] // c["cb"])
-    n = min(ncb, max(threads * 8, 128))
+    # size each step's sample so that warm-up + timed steps take ~60 s in all
+    n0 = min(ncb, max(threads * 8, 128))
+    t0 = time.perf_counter()
+    s = oracle.encode(img, lut_np, c["passes"], c["levels"], c["cb"], threads, cb_range=(0, n0))
+    oracle.decode(s, img.shape, lut_np, c["passes"], c["levels"], c["cb"], threads, cb_range=(0, n0))
+    t_n0 = max(time.perf_counter() - t0, 1e-4)
+    budget = 60.0 / max(1, args.warmup + args.steps)
+    n = int(max(min(n0, ncb), min(ncb, n0 * budget / t_n0)))
     times = []
     for k in range(args.warmup + args.steps):
         t0 = time.perf_counter()
@@ -287,7 +297,7 @@ def run_ours(args, c):
         "e2e": {"value": e2e, "unit": "Gcoeff/s", "h2d_bytes_per_step": 2 * 4 * N, "d2h_bytes_per_step": 2 * 4 * N + 8},
         "gpu_launches": 2 * args.steps,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": None, "peak_source": peak_kind,
+                     "traffic": NCU_TRAFFIC.get(args.config), "peak_source": peak_kind,
                      "kernel": "k_bpc decoder" if td1 >= te1 else "k_bpc encoder",
                      "note": "8 B/coefficient algorithmic; the coder is bound by SM integer issue, not HBM"},
         "clocks": clk.summary(), "wall_s_timed": wall,
@@ -306,7 +316,7 @@ def run_ours(args, c):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="cfg2", choices=sorted(CONFIGS))
