@@ -178,3 +178,98 @@ def decode_device(stream_in, coeffs_out, lut: DeviceLut, cb: int = 64, status=No
     _check(lib().bpc_decode_device(_ptr(stream_in), _ptr(coeffs_out), X, Y, ctypes.c_void_p(lut.ptr), lut.n,
                                    lut.passes, lut.levels, cb, ctypes.c_void_p(_ptr(status)),
                                    ctypes.c_void_p(_ptr(counts)), grid, ctypes.c_void_p(s)), "bpc_decode_device")
+
+
+# ------------------------------------------------------------ batched form
+class Batch:
+    """Batched persistent coding of many images (bpc_batch_* in the C ABI).
+
+    images: list of (X, Y, levels, passes, cb); luts: dict passes -> folder.
+    Device tensors are torch int32; the compact container is one int32 tensor
+    plus int64 offsets (codeblocks + 1 entries)."""
+
+    def __init__(self, images, luts: dict):
+        import torch
+        L = lib()
+        vp, ip = ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)
+        L.bpc_batch_create.argtypes = [ctypes.c_int, ip, ip, ip, ip, ip, ctypes.POINTER(vp), ip, ctypes.POINTER(vp)]
+        L.bpc_batch_codeblocks.argtypes = [vp]
+        L.bpc_batch_codeblocks.restype = ctypes.c_longlong
+        L.bpc_batch_words.argtypes = [vp]
+        L.bpc_batch_words.restype = ctypes.c_longlong
+        L.bpc_batch_encode.argtypes = [vp, ctypes.POINTER(vp), vp, vp, vp, vp]
+        L.bpc_batch_decode.argtypes = [vp, vp, vp, ctypes.POINTER(vp), vp, vp]
+        L.bpc_batch_set_schedule.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+        L.bpc_batch_get_schedule.argtypes = [vp, ip, ip, ip, ip]
+        L.bpc_batch_tune.argtypes = [vp, ctypes.POINTER(vp), vp, vp, ctypes.POINTER(vp), vp,
+                                     ctypes.POINTER(ctypes.c_double)]
+        L.bpc_batch_destroy.argtypes = [vp]
+        self.images = list(images)
+        n = len(self.images)
+        arr = lambda k: (ctypes.c_int * n)(*[im[k] for im in self.images])
+        self._luts = {}
+        lut_ptrs, lut_ns = [], []
+        for (_, _, lv, ps, _) in self.images:
+            if (ps, lv) not in self._luts:
+                self._luts[(ps, lv)] = DeviceLut(luts[ps], ps, lv)
+            d = self._luts[(ps, lv)]
+            lut_ptrs.append(d.ptr)
+            lut_ns.append(d.n)
+        h = vp()
+        _check(L.bpc_batch_create(n, arr(0), arr(1), arr(2), arr(3), arr(4), (vp * n)(*lut_ptrs),
+                                  (ctypes.c_int * n)(*lut_ns), ctypes.byref(h)), "bpc_batch_create")
+        self.h = h
+        self.codeblocks = L.bpc_batch_codeblocks(h)
+        self.words = L.bpc_batch_words(h)
+        self.torch = torch
+
+    def _ptrs(self, tensors):
+        return (ctypes.c_void_p * len(tensors))(*[t.data_ptr() for t in tensors])
+
+    def encode(self, coeffs, compact, offsets, status=None, stream=None):
+        s = self.torch.cuda.current_stream().cuda_stream if stream is None else stream
+        _check(lib().bpc_batch_encode(self.h, self._ptrs(coeffs), compact.data_ptr(), offsets.data_ptr(),
+                                      None if status is None else status.data_ptr(), s), "bpc_batch_encode")
+
+    def decode(self, compact, offsets, out, status=None, stream=None):
+        s = self.torch.cuda.current_stream().cuda_stream if stream is None else stream
+        _check(lib().bpc_batch_decode(self.h, compact.data_ptr(), offsets.data_ptr(), self._ptrs(out),
+                                      None if status is None else status.data_ptr(), s), "bpc_batch_decode")
+
+    def set_schedule(self, ctas_enc: int, ctas_dec: int, per_item: int, graph: bool = True) -> None:
+        _check(lib().bpc_batch_set_schedule(self.h, ctas_enc, ctas_dec, per_item, int(graph)), "set_schedule")
+
+    def schedule(self):
+        a, b, c, d = (ctypes.c_int() for _ in range(4))
+        lib().bpc_batch_get_schedule(self.h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c), ctypes.byref(d))
+        return a.value, b.value, c.value, bool(d.value)
+
+    def tune(self, coeffs, compact, offsets, out) -> float:
+        us = ctypes.c_double()
+        s = self.torch.cuda.current_stream().cuda_stream
+        _check(lib().bpc_batch_tune(self.h, self._ptrs(coeffs), compact.data_ptr(), offsets.data_ptr(),
+                                    self._ptrs(out), s, ctypes.byref(us)), "bpc_batch_tune")
+        return us.value
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().bpc_batch_destroy(self.h)
+            self.h = None
+        for d in self._luts.values():
+            d.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def slots_to_compact(stream: np.ndarray, cb: int) -> list:
+    """Per-codeblock [MSB, codewords...] word lists of a slot stream."""
+    s = np.asarray(stream).reshape(-1, cb * cb)
+    out = []
+    for row in s:
+        n = int(np.count_nonzero(row[1:] != -1))
+        out.append(row[:1 + n])
+    return out

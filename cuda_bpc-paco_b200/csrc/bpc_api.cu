@@ -66,6 +66,7 @@ int fill_params(bpc::Params &p, const int *in, int *out, int X, int Y, const int
     p.cp_off = o.cp_off;
     p.status = d_status;
     p.counts = d_counts;
+    p.offsets = nullptr;
     return BPC_OK;
 }
 

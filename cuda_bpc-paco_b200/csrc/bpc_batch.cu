@@ -1,0 +1,610 @@
+// bpc_batch.cu -- batched persistent coding of many images of mixed size, DWT
+// depth, pass count and codeblock size.
+//
+// Layout.  The batch's codeblocks are numbered image by image (image i's
+// codeblock k is batch codeblock cb_base[i] + k).  Encoding writes each image's
+// slot stream into batch scratch (the plain kernel's layout), then a prefix scan
+// over (codewords + 1) per codeblock gives offsets and a gather copies each
+// codeblock's MSB word and codewords into one compact container:
+//   compact[offsets[g] .. offsets[g+1]) = MSB, codeword 1, ..., codeword n.
+// Decoding reads the container directly (the decoder's codeword ring treats the
+// words past a codeblock's end as the slot's -1 fill, so the result is the same
+// as decoding the slot stream).
+//
+// Schedule.  One persistent kernel per (passes, codeblock size) class; the
+// classes run concurrently on forked streams.  Warps pull work items (image,
+// run of codeblocks) from a device queue with an atomic counter; items are
+// ordered coarse subbands first (their codeblocks have more bitplanes).  The
+// whole encode (queue reset, four kernels, scan, gather) or decode is captured
+// in one CUDA graph per set of buffer pointers and replayed.  The grid size
+// (CTAs per SM) and codeblocks per item are picked by bpc_batch_tune.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cub/device/device_scan.cuh>
+#include <map>
+#include <vector>
+
+#include "../../include/bpc_paco.h"
+#include "bpc_core.cuh"
+#include "bpc_kernels.h"
+
+namespace bpc {
+
+struct BatchImage {
+    const int32_t *in;  // encode: coefficients; decode: compact container base
+    int32_t *out;       // encode: slot scratch of this image; decode: coefficients
+    const uint8_t *tab; // LUT bytes (global, L1-resident)
+    int X, Y, levels, cbs, ncbx, ncb;
+    int a_sig, a_sign, cp_off;
+    long long cb_base;
+};
+
+struct BatchItem {
+    int image, cb0, n;
+};
+
+struct GpuWarpB {
+    __device__ __forceinline__ int lane() const { return (int)(threadIdx.x & 31u); }
+    __device__ __forceinline__ uint32_t ballot(bool p) { return __ballot_sync(0xffffffffu, p); }
+    __device__ __forceinline__ bool any(bool p) { return __any_sync(0xffffffffu, p) != 0; }
+    __device__ __forceinline__ uint32_t shfl_xor(uint32_t v, int o) { return __shfl_xor_sync(0xffffffffu, v, o); }
+    __device__ __forceinline__ uint32_t shfl_up(uint32_t v, int d) { return __shfl_up_sync(0xffffffffu, v, d); }
+    __device__ __forceinline__ uint32_t shfl_down(uint32_t v, int d) { return __shfl_down_sync(0xffffffffu, v, d); }
+    __device__ __forceinline__ uint32_t shfl_idx(uint32_t v, int l) { return __shfl_sync(0xffffffffu, v, l); }
+    __device__ __forceinline__ void smem_or(uint32_t *p, uint32_t v) { atomicOr(p, v); }
+    __device__ __forceinline__ void sync() { __syncwarp(); }
+    __device__ __forceinline__ void syncmask(uint32_t m) { __syncwarp(m); }
+    __device__ __forceinline__ void load2(const int32_t *p, int32_t &a, int32_t &b) {
+        const int2 v = __ldg(reinterpret_cast<const int2 *>(p));
+        a = v.x;
+        b = v.y;
+    }
+    __device__ __forceinline__ int32_t load1(const int32_t *p) { return __ldg(p); }
+    __device__ __forceinline__ void store1(int32_t *p, int32_t a) { *p = a; }
+    __device__ __forceinline__ void store2(int32_t *p, int32_t a, int32_t b) {
+        *reinterpret_cast<int2 *>(p) = make_int2(a, b);
+    }
+    __device__ __forceinline__ void load4(const int32_t *p, uint32_t &a, uint32_t &b, uint32_t &c, uint32_t &d) {
+        const int4 v = __ldg(reinterpret_cast<const int4 *>(p));
+        a = (uint32_t)v.x;
+        b = (uint32_t)v.y;
+        c = (uint32_t)v.z;
+        d = (uint32_t)v.w;
+    }
+    __device__ __forceinline__ void atomic_or(int *p, int v) { atomicOr(p, v); }
+};
+
+// LUT (ints) -> byte table zero-padded to tab_n, flagging entries outside 0..255
+__global__ void k_lut_bytes(const int *lut, int lut_n, uint8_t *tab, int tab_n, int *status) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < tab_n; k += gridDim.x * blockDim.x) {
+        int v = k < lut_n ? lut[k] : 0;
+        if (v < 0 || v > 255) {
+            if (status) atomicOr(status, ST_LUT_RANGE);
+            v = 0;
+        }
+        tab[k] = (uint8_t)v;
+    }
+}
+
+template <int PASSES, int CBS, bool ENC>
+__global__ void __launch_bounds__(kWarps * 32, ENC ? kMinCtasEnc : kMinCtasDec)
+    k_bpc_batch(const BatchImage *imgs, const BatchItem *items, int nitems, unsigned *head, int *counts,
+                const long long *offsets, int *status) {
+    using G = Geo<CBS>;
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int warp = (int)(threadIdx.x >> 5);
+    uint32_t *ring = reinterpret_cast<uint32_t *>(smem) + warp * (ENC ? 512 : G::RING_WORDS);
+    GpuWarpB w;
+    uint32_t planes[28][4];
+    uint8_t ev_key[ENC ? 256 : 1];
+    uint32_t ev_val[ENC ? 256 : 1];
+    for (;;) {
+        unsigned it = 0;
+        if (w.lane() == 0) it = atomicAdd(head, 1u);
+        it = w.shfl_idx(it, 0);
+        if (it >= (unsigned)nitems) break;
+        const BatchItem item = items[it];
+        const BatchImage im = imgs[item.image];
+        Params p;
+        p.in = im.in;
+        p.out = im.out;
+        p.lut = nullptr;
+        p.lut_n = 0;
+        p.tab_n = 0;
+        p.X = im.X;
+        p.Y = im.Y;
+        p.levels = im.levels;
+        p.ncbx = im.ncbx;
+        p.ncb = im.ncb;
+        p.a_sig = im.a_sig;
+        p.a_sign = im.a_sign;
+        p.cp_off = im.cp_off;
+        p.status = status;
+        p.counts = counts ? counts + im.cb_base : nullptr;
+        p.offsets = offsets ? offsets + im.cb_base : nullptr;
+        for (int k = 0; k < item.n; k += G::NG) {
+            Coder<PASSES, CBS, ENC, GpuWarpB> cd(w, p, ring, im.tab, planes, ev_key, ev_val);
+            cd.run(item.cb0 + k);
+        }
+    }
+}
+
+// words per codeblock in the container: MSB + codewords, capped at the slot
+__global__ void k_sizes(const int *counts, const int *cap_of, long long ncb, long long *sizes) {
+    for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < ncb;
+         g += (long long)gridDim.x * blockDim.x) {
+        const long long n = (long long)counts[g] + 1;
+        const long long c = cap_of[g] ? (long long)cap_of[g] : 4096;
+        sizes[g] = n < c ? n : c;
+    }
+}
+
+// copy each codeblock's words from the slot scratch into the container
+__global__ void k_gather(const BatchImage *imgs, int nimg, const long long *offsets, long long ncb,
+                         const int32_t *const *slots_of, int32_t *compact) {
+    const long long warp = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+    for (long long g = warp; g < ncb; g += nw) {
+        int lo = 0, hi = nimg - 1;
+        while (lo < hi) {  // last image with cb_base <= g
+            const int mid = (lo + hi + 1) >> 1;
+            if (imgs[mid].cb_base <= g)
+                lo = mid;
+            else
+                hi = mid - 1;
+        }
+        const BatchImage &im = imgs[lo];
+        const long long k = g - im.cb_base;
+        const int32_t *src = slots_of[lo] + k * (long long)(im.cbs * im.cbs);
+        const long long o0 = offsets[g], n = offsets[g + 1] - o0;
+        for (long long q = lane; q < n; q += 32) compact[o0 + q] = src[q];
+    }
+}
+
+}  // namespace bpc
+
+using namespace bpc;
+
+namespace {
+
+#define CUDA_TRY(x)                                                                       \
+    do {                                                                                  \
+        cudaError_t e_ = (x);                                                             \
+        if (e_ != cudaSuccess) {                                                          \
+            std::fprintf(stderr, "bpc batch: %s failed: %s\n", #x, cudaGetErrorString(e_)); \
+            return BPC_ERR_CUDA;                                                          \
+        }                                                                                 \
+    } while (0)
+
+constexpr int kClasses = 4;  // (passes 2|3) x (codeblock 64|32)
+inline int class_of(int passes, int cb) { return (passes == 3 ? 2 : 0) + (cb == 32 ? 1 : 0); }
+
+struct Graph {
+    cudaGraphExec_t exec = nullptr;
+    std::vector<const void *> key;
+};
+
+struct Batch {
+    int n = 0;
+    std::vector<int> X, Y, levels, passes, cb;
+    std::vector<long long> cb_base;
+    long long ncb = 0, words = 0;
+    std::vector<const uint8_t *> tab_of;  // per image
+    std::vector<uint8_t *> tabs;          // owned byte tables
+    std::vector<int32_t *> slots;         // owned slot scratch per image
+    // device
+    BatchImage *d_imgs_enc = nullptr, *d_imgs_dec = nullptr;
+    BatchItem *d_items[kClasses] = {};
+    int nitems[kClasses] = {};
+    std::vector<BatchItem> h_items[kClasses];
+    unsigned *d_head = nullptr;  // kClasses counters
+    int *d_counts = nullptr, *d_cap = nullptr;
+    long long *d_sizes = nullptr;
+    int32_t **d_slots = nullptr;
+    void *d_scan_tmp = nullptr;
+    size_t scan_tmp_bytes = 0;
+    int sms = 148;
+    // schedule
+    int ctas_enc = kMinCtasEnc, ctas_dec = kMinCtasDec, per_item = 4, use_graph = 1;
+    cudaStream_t side[kClasses - 1] = {};
+    cudaEvent_t ev_fork = nullptr, ev_join[kClasses - 1] = {};
+    Graph genc, gdec;
+};
+
+int build_items(Batch &b) {
+    for (int c = 0; c < kClasses; c++) b.h_items[c].clear();
+    struct Tmp {
+        BatchItem it;
+        int weight;
+    };
+    std::vector<Tmp> tmp[kClasses];
+    for (int i = 0; i < b.n; i++) {
+        const int cbs = b.cb[i], ncbx = b.X[i] / cbs, ncb = ncbx * (b.Y[i] / cbs);
+        const int ng = cbs == 64 ? 1 : 2;
+        const int step = std::max(ng, (b.per_item + ng - 1) / ng * ng);
+        for (int k = 0; k < ncb; k += step) {
+            // coarse subbands first: level of the run's first codeblock
+            const int x = (k % ncbx) * cbs, y = (k / ncbx) * cbs;
+            int lvl = b.levels[i];
+            for (int a = 1; a <= b.levels[i]; a++)
+                if (x >= (b.X[i] >> a) || y >= (b.Y[i] >> a)) {
+                    lvl = a - 1;
+                    break;
+                }
+            tmp[class_of(b.passes[i], cbs)].push_back({{i, k, std::min(step, ncb - k)}, lvl});
+        }
+    }
+    for (int c = 0; c < kClasses; c++) {
+        std::stable_sort(tmp[c].begin(), tmp[c].end(), [](const Tmp &a, const Tmp &z) { return a.weight > z.weight; });
+        for (auto &t : tmp[c]) b.h_items[c].push_back(t.it);
+        b.nitems[c] = (int)b.h_items[c].size();
+        cudaFree(b.d_items[c]);
+        b.d_items[c] = nullptr;
+        if (b.nitems[c]) {
+            CUDA_TRY(cudaMalloc((void **)&b.d_items[c], b.nitems[c] * sizeof(BatchItem)));
+            CUDA_TRY(cudaMemcpy(b.d_items[c], b.h_items[c].data(), b.nitems[c] * sizeof(BatchItem),
+                                cudaMemcpyHostToDevice));
+        }
+    }
+    return BPC_OK;
+}
+
+template <int PASSES, int CBS, bool ENC>
+cudaError_t launch_batch(const Batch &b, int cls, const BatchImage *imgs, const long long *offsets, int *status,
+                         cudaStream_t st) {
+    using G = Geo<CBS>;
+    const size_t sm = (size_t)kWarps * 4u * (size_t)(ENC ? 512 : G::RING_WORDS);
+    cudaError_t e = cudaFuncSetAttribute(k_bpc_batch<PASSES, CBS, ENC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)sm);
+    if (e != cudaSuccess) return e;
+    const int grid = std::max(1, std::min(b.sms * (ENC ? b.ctas_enc : b.ctas_dec),
+                                          (b.nitems[cls] + kWarps - 1) / kWarps));
+    k_bpc_batch<PASSES, CBS, ENC><<<grid, kWarps * 32, sm, st>>>(imgs, b.d_items[cls], b.nitems[cls], b.d_head + cls,
+                                                                 ENC ? b.d_counts : nullptr, offsets, status);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_class(const Batch &b, int cls, bool enc, const BatchImage *imgs, const long long *offsets,
+                         int *status, cudaStream_t st) {
+    if (b.nitems[cls] == 0) return cudaSuccess;
+    switch (cls) {
+        case 0: return enc ? launch_batch<2, 64, true>(b, cls, imgs, offsets, status, st)
+                           : launch_batch<2, 64, false>(b, cls, imgs, offsets, status, st);
+        case 1: return enc ? launch_batch<2, 32, true>(b, cls, imgs, offsets, status, st)
+                           : launch_batch<2, 32, false>(b, cls, imgs, offsets, status, st);
+        case 2: return enc ? launch_batch<3, 64, true>(b, cls, imgs, offsets, status, st)
+                           : launch_batch<3, 64, false>(b, cls, imgs, offsets, status, st);
+        default: return enc ? launch_batch<3, 32, true>(b, cls, imgs, offsets, status, st)
+                            : launch_batch<3, 32, false>(b, cls, imgs, offsets, status, st);
+    }
+}
+
+// enqueue one whole encode or decode on `st` (forks the classes onto side streams)
+int enqueue(Batch &b, bool enc, const BatchImage *imgs, int32_t *compact, const long long *offsets_in,
+            long long *offsets_out, int *status, cudaStream_t st) {
+    CUDA_TRY(cudaMemsetAsync(b.d_head, 0, kClasses * sizeof(unsigned), st));
+    CUDA_TRY(cudaEventRecord(b.ev_fork, st));
+    int used = 0;
+    for (int c = 0; c < kClasses; c++) {
+        if (!b.nitems[c]) continue;
+        cudaStream_t s = st;
+        if (used > 0) {
+            s = b.side[used - 1];
+            CUDA_TRY(cudaStreamWaitEvent(s, b.ev_fork, 0));
+        }
+        CUDA_TRY(launch_class(b, c, enc, imgs, enc ? nullptr : offsets_in, status, s));
+        if (used > 0) CUDA_TRY(cudaEventRecord(b.ev_join[used - 1], s));
+        used++;
+    }
+    for (int k = 0; k + 1 < used; k++) CUDA_TRY(cudaStreamWaitEvent(st, b.ev_join[k], 0));
+    if (enc) {
+        const int threads = 256;
+        const int blocks = (int)std::min<long long>((b.ncb + threads - 1) / threads, 4096);
+        k_sizes<<<blocks, threads, 0, st>>>(b.d_counts, b.d_cap, b.ncb, b.d_sizes);
+        CUDA_TRY(cudaGetLastError());
+        CUDA_TRY(cudaMemsetAsync(offsets_out, 0, sizeof(long long), st));
+        size_t tmp = b.scan_tmp_bytes;
+        CUDA_TRY(cub::DeviceScan::InclusiveSum(b.d_scan_tmp, tmp, b.d_sizes, offsets_out + 1, (int)b.ncb, st));
+        const int gb = (int)std::min<long long>((b.ncb * 32 + 255) / 256, 148 * 16);
+        k_gather<<<gb, 256, 0, st>>>(imgs, b.n, offsets_out, b.ncb, b.d_slots, compact);
+        CUDA_TRY(cudaGetLastError());
+    }
+    return BPC_OK;
+}
+
+int run(Batch &b, bool enc, const BatchImage *h_imgs, int32_t *compact, const long long *offsets_in,
+        long long *offsets_out, int *status, cudaStream_t st) {
+    BatchImage *d_imgs = enc ? b.d_imgs_enc : b.d_imgs_dec;
+    Graph &gr = enc ? b.genc : b.gdec;
+    std::vector<const void *> key;
+    for (int i = 0; i < b.n; i++) {
+        key.push_back(h_imgs[i].in);
+        key.push_back(h_imgs[i].out);
+    }
+    key.push_back(compact);
+    key.push_back(offsets_in);
+    key.push_back(offsets_out);
+    key.push_back(status);
+    key.push_back(st);
+    if (!b.use_graph) {
+        CUDA_TRY(cudaMemcpyAsync(d_imgs, h_imgs, b.n * sizeof(BatchImage), cudaMemcpyHostToDevice, st));
+        return enqueue(b, enc, d_imgs, compact, offsets_in, offsets_out, status, st);
+    }
+    if (!gr.exec || gr.key != key) {
+        if (gr.exec) cudaGraphExecDestroy(gr.exec);
+        gr.exec = nullptr;
+        // descriptors are constant for this key: upload before capturing
+        CUDA_TRY(cudaMemcpyAsync(d_imgs, h_imgs, b.n * sizeof(BatchImage), cudaMemcpyHostToDevice, st));
+        CUDA_TRY(cudaStreamSynchronize(st));
+        cudaStream_t cap;
+        CUDA_TRY(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+        cudaGraph_t g;
+        CUDA_TRY(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
+        const int rc = enqueue(b, enc, d_imgs, compact, offsets_in, offsets_out, status, cap);
+        cudaError_t e = cudaStreamEndCapture(cap, &g);
+        cudaStreamDestroy(cap);
+        if (rc) return rc;
+        if (e != cudaSuccess) {
+            std::fprintf(stderr, "bpc batch: capture failed: %s\n", cudaGetErrorString(e));
+            return BPC_ERR_CUDA;
+        }
+        e = cudaGraphInstantiate(&gr.exec, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) {
+            std::fprintf(stderr, "bpc batch: instantiate failed: %s\n", cudaGetErrorString(e));
+            return BPC_ERR_CUDA;
+        }
+        gr.key = key;
+    }
+    CUDA_TRY(cudaGraphLaunch(gr.exec, st));
+    return BPC_OK;
+}
+
+void image_desc(const Batch &b, int i, BatchImage &im) {
+    const int cbs = b.cb[i];
+    const LutOffsets o = lut_offsets(b.levels[i], b.passes[i], 1);
+    im.tab = b.tab_of[i];
+    im.X = b.X[i];
+    im.Y = b.Y[i];
+    im.levels = b.levels[i];
+    im.cbs = cbs;
+    im.ncbx = b.X[i] / cbs;
+    im.ncb = im.ncbx * (b.Y[i] / cbs);
+    im.a_sig = o.a_sig;
+    im.a_sign = o.a_sign;
+    im.cp_off = o.cp_off;
+    im.cb_base = b.cb_base[i];
+}
+
+void free_batch(Batch *b) {
+    if (!b) return;
+    for (auto *t : b->tabs) cudaFree(t);
+    for (auto *s : b->slots) cudaFree(s);
+    for (int c = 0; c < kClasses; c++) cudaFree(b->d_items[c]);
+    cudaFree(b->d_imgs_enc);
+    cudaFree(b->d_imgs_dec);
+    cudaFree(b->d_head);
+    cudaFree(b->d_counts);
+    cudaFree(b->d_cap);
+    cudaFree(b->d_sizes);
+    cudaFree(b->d_slots);
+    cudaFree(b->d_scan_tmp);
+    for (int k = 0; k < kClasses - 1; k++) {
+        if (b->side[k]) cudaStreamDestroy(b->side[k]);
+        if (b->ev_join[k]) cudaEventDestroy(b->ev_join[k]);
+    }
+    if (b->ev_fork) cudaEventDestroy(b->ev_fork);
+    if (b->genc.exec) cudaGraphExecDestroy(b->genc.exec);
+    if (b->gdec.exec) cudaGraphExecDestroy(b->gdec.exec);
+    delete b;
+}
+
+int create(Batch &b, int n, const int *X, const int *Y, const int *levels, const int *passes, const int *cbsz,
+           const int *const *d_luts, const int *lut_n) {
+    b.n = n;
+    std::map<std::pair<const int *, int>, uint8_t *> tab_cache;
+    for (int i = 0; i < n; i++) {
+        if ((passes[i] != 2 && passes[i] != 3) || (cbsz[i] != 64 && cbsz[i] != 32) || levels[i] < 1 ||
+            levels[i] > 16 || X[i] <= 0 || Y[i] <= 0 || X[i] % cbsz[i] || Y[i] % cbsz[i] || !d_luts[i] ||
+            lut_n[i] <= 0)
+            return BPC_ERR_ARG;
+        b.X.push_back(X[i]);
+        b.Y.push_back(Y[i]);
+        b.levels.push_back(levels[i]);
+        b.passes.push_back(passes[i]);
+        b.cb.push_back(cbsz[i]);
+        b.cb_base.push_back(b.ncb);
+        b.ncb += (long long)(X[i] / cbsz[i]) * (Y[i] / cbsz[i]);
+        b.words += (long long)X[i] * Y[i];
+        const int tab_n = lut_offsets(levels[i], passes[i], lut_n[i]).tab_n;
+        auto key = std::make_pair(d_luts[i], tab_n);
+        auto it = tab_cache.find(key);
+        if (it == tab_cache.end()) {
+            uint8_t *t = nullptr;
+            CUDA_TRY(cudaMalloc((void **)&t, tab_n));
+            b.tabs.push_back(t);
+            k_lut_bytes<<<(tab_n + 255) / 256, 256>>>(d_luts[i], lut_n[i], t, tab_n, nullptr);
+            CUDA_TRY(cudaGetLastError());
+            it = tab_cache.emplace(key, t).first;
+        }
+        b.tab_of.push_back(it->second);
+    }
+    int dev = 0;
+    CUDA_TRY(cudaGetDevice(&dev));
+    CUDA_TRY(cudaDeviceGetAttribute(&b.sms, cudaDevAttrMultiProcessorCount, dev));
+    std::vector<int32_t *> h_slots;
+    std::vector<int> h_cap((size_t)b.ncb);
+    for (int i = 0; i < n; i++) {
+        int32_t *s = nullptr;
+        CUDA_TRY(cudaMalloc((void **)&s, (size_t)X[i] * Y[i] * sizeof(int32_t)));
+        b.slots.push_back(s);
+        h_slots.push_back(s);
+        const long long nb = (long long)(X[i] / cbsz[i]) * (Y[i] / cbsz[i]);
+        for (long long k = 0; k < nb; k++) h_cap[(size_t)(b.cb_base[i] + k)] = cbsz[i] * cbsz[i];
+    }
+    CUDA_TRY(cudaMalloc((void **)&b.d_imgs_enc, n * sizeof(BatchImage)));
+    CUDA_TRY(cudaMalloc((void **)&b.d_imgs_dec, n * sizeof(BatchImage)));
+    CUDA_TRY(cudaMalloc((void **)&b.d_head, kClasses * sizeof(unsigned)));
+    CUDA_TRY(cudaMalloc((void **)&b.d_counts, b.ncb * sizeof(int)));
+    CUDA_TRY(cudaMalloc((void **)&b.d_cap, b.ncb * sizeof(int)));
+    CUDA_TRY(cudaMemcpy(b.d_cap, h_cap.data(), b.ncb * sizeof(int), cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMalloc((void **)&b.d_sizes, b.ncb * sizeof(long long)));
+    CUDA_TRY(cudaMalloc((void **)&b.d_slots, n * sizeof(int32_t *)));
+    CUDA_TRY(cudaMemcpy(b.d_slots, h_slots.data(), n * sizeof(int32_t *), cudaMemcpyHostToDevice));
+    b.scan_tmp_bytes = 0;
+    CUDA_TRY(cub::DeviceScan::InclusiveSum(nullptr, b.scan_tmp_bytes, b.d_sizes, (long long *)nullptr, (int)b.ncb));
+    CUDA_TRY(cudaMalloc(&b.d_scan_tmp, b.scan_tmp_bytes + 16));
+    for (int k = 0; k < kClasses - 1; k++) {
+        CUDA_TRY(cudaStreamCreateWithFlags(&b.side[k], cudaStreamNonBlocking));
+        CUDA_TRY(cudaEventCreateWithFlags(&b.ev_join[k], cudaEventDisableTiming));
+    }
+    CUDA_TRY(cudaEventCreateWithFlags(&b.ev_fork, cudaEventDisableTiming));
+    CUDA_TRY(cudaDeviceSynchronize());
+    return build_items(b);
+}
+
+}  // namespace
+
+extern "C" {
+
+int bpc_batch_create(int n_images, const int *X, const int *Y, const int *levels, const int *passes,
+                     const int *cb_size, const int *const *d_luts, const int *lut_n, void **batch) {
+    if (!batch || n_images <= 0 || !X || !Y || !levels || !passes || !cb_size || !d_luts || !lut_n) return BPC_ERR_ARG;
+    *batch = nullptr;
+    Batch *b = new Batch();
+    const int rc = create(*b, n_images, X, Y, levels, passes, cb_size, d_luts, lut_n);
+    if (rc) {
+        free_batch(b);
+        return rc;
+    }
+    *batch = b;
+    return BPC_OK;
+}
+
+long long bpc_batch_codeblocks(const void *batch) { return batch ? ((const Batch *)batch)->ncb : BPC_ERR_ARG; }
+
+long long bpc_batch_words(const void *batch) { return batch ? ((const Batch *)batch)->words : BPC_ERR_ARG; }
+
+int bpc_batch_set_schedule(void *batch, int ctas_per_sm_enc, int ctas_per_sm_dec, int cbs_per_item, int use_graph) {
+    Batch *b = (Batch *)batch;
+    if (!b || ctas_per_sm_enc < 1 || ctas_per_sm_enc > kMinCtasEnc || ctas_per_sm_dec < 1 ||
+        ctas_per_sm_dec > kMinCtasDec || cbs_per_item < 1 || cbs_per_item > 64)
+        return BPC_ERR_ARG;
+    b->ctas_enc = ctas_per_sm_enc;
+    b->ctas_dec = ctas_per_sm_dec;
+    b->use_graph = use_graph ? 1 : 0;
+    if (cbs_per_item != b->per_item) {
+        b->per_item = cbs_per_item;
+        const int rc = build_items(*b);
+        if (rc) return rc;
+    }
+    if (b->genc.exec) cudaGraphExecDestroy(b->genc.exec);
+    if (b->gdec.exec) cudaGraphExecDestroy(b->gdec.exec);
+    b->genc.exec = b->gdec.exec = nullptr;
+    return BPC_OK;
+}
+
+int bpc_batch_get_schedule(const void *batch, int *ctas_per_sm_enc, int *ctas_per_sm_dec, int *cbs_per_item,
+                           int *use_graph) {
+    const Batch *b = (const Batch *)batch;
+    if (!b) return BPC_ERR_ARG;
+    if (ctas_per_sm_enc) *ctas_per_sm_enc = b->ctas_enc;
+    if (ctas_per_sm_dec) *ctas_per_sm_dec = b->ctas_dec;
+    if (cbs_per_item) *cbs_per_item = b->per_item;
+    if (use_graph) *use_graph = b->use_graph;
+    return BPC_OK;
+}
+
+int bpc_batch_encode(void *batch, const int *const *d_coeffs, int *d_compact, long long *d_offsets, int *d_status,
+                     void *stream) {
+    Batch *b = (Batch *)batch;
+    if (!b || !d_coeffs || !d_compact || !d_offsets) return BPC_ERR_ARG;
+    std::vector<BatchImage> h(b->n);
+    for (int i = 0; i < b->n; i++) {
+        if (!d_coeffs[i]) return BPC_ERR_ARG;
+        image_desc(*b, i, h[i]);
+        h[i].in = d_coeffs[i];
+        h[i].out = b->slots[i];
+    }
+    return run(*b, true, h.data(), d_compact, nullptr, d_offsets, d_status, (cudaStream_t)stream);
+}
+
+int bpc_batch_decode(void *batch, const int *d_compact, const long long *d_offsets, int *const *d_coeffs,
+                     int *d_status, void *stream) {
+    Batch *b = (Batch *)batch;
+    if (!b || !d_coeffs || !d_compact || !d_offsets) return BPC_ERR_ARG;
+    std::vector<BatchImage> h(b->n);
+    for (int i = 0; i < b->n; i++) {
+        if (!d_coeffs[i]) return BPC_ERR_ARG;
+        image_desc(*b, i, h[i]);
+        h[i].in = d_compact;
+        h[i].out = d_coeffs[i];
+    }
+    return run(*b, false, h.data(), nullptr, d_offsets, nullptr, d_status, (cudaStream_t)stream);
+}
+
+// Autotuner: time encode and decode under each schedule on the caller's
+// buffers and keep the fastest (codeblocks per work item shared by both
+// directions, CTAs per SM per direction).  Returns the best total in us.
+int bpc_batch_tune(void *batch, const int *const *d_coeffs, int *d_compact, long long *d_offsets, int *const *d_out,
+                   void *stream, double *best_us) {
+    Batch *b = (Batch *)batch;
+    if (!b) return BPC_ERR_ARG;
+    cudaStream_t st = (cudaStream_t)stream;
+    cudaEvent_t e0, e1;
+    CUDA_TRY(cudaEventCreate(&e0));
+    CUDA_TRY(cudaEventCreate(&e1));
+    const int items[] = {1, 2, 4, 8};
+    double best = 1e30;
+    int bi = b->per_item, be = b->ctas_enc, bd = b->ctas_dec;
+    auto timed = [&](bool enc, float &ms) -> int {
+        float acc = 0.f;
+        for (int r = 0; r < 3; r++) {
+            CUDA_TRY(cudaEventRecord(e0, st));
+            const int rc = enc ? bpc_batch_encode(batch, d_coeffs, d_compact, d_offsets, nullptr, stream)
+                               : bpc_batch_decode(batch, d_compact, d_offsets, d_out, nullptr, stream);
+            if (rc) return rc;
+            CUDA_TRY(cudaEventRecord(e1, st));
+            CUDA_TRY(cudaEventSynchronize(e1));
+            float t;
+            CUDA_TRY(cudaEventElapsedTime(&t, e0, e1));
+            if (r) acc += t;  // the first run may capture the graph
+        }
+        ms = acc / 2.f;
+        return BPC_OK;
+    };
+    for (int it : items) {
+        float te_best = 1e30f, td_best = 1e30f;
+        int ce = kMinCtasEnc, cd = kMinCtasDec;
+        for (int c = 1; c <= kMinCtasEnc; c++) {
+            int rc = bpc_batch_set_schedule(batch, c, b->ctas_dec, it, b->use_graph);
+            if (rc) return rc;
+            float t;
+            if ((rc = timed(true, t))) return rc;
+            if (t < te_best) te_best = t, ce = c;
+        }
+        for (int c = 2; c <= kMinCtasDec; c++) {
+            int rc = bpc_batch_set_schedule(batch, ce, c, it, b->use_graph);
+            if (rc) return rc;
+            float t;
+            if ((rc = timed(false, t))) return rc;
+            if (t < td_best) td_best = t, cd = c;
+        }
+        if (te_best + td_best < best) best = te_best + td_best, bi = it, be = ce, bd = cd;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (best_us) *best_us = best * 1e3;
+    return bpc_batch_set_schedule(batch, be, bd, bi, b->use_graph);
+}
+
+int bpc_batch_destroy(void *batch) {
+    free_batch((Batch *)batch);
+    return BPC_OK;
+}
+
+}  // extern "C"

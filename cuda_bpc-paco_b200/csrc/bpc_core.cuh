@@ -56,6 +56,9 @@ struct Params {
     int a_sig, a_sign, cp_off;  // LUT section offsets as the reference kernel forms them
     int *status;         // OR of ST_* bits, may be null
     int *counts;         // per-codeblock codeword count, may be null
+    // decoder input in the compact container: codeblock k's words (MSB and
+    // codewords) are in[offsets[k] .. offsets[k+1]); null = slot layout
+    const long long *offsets;
 };
 
 // LUT offsets the reference kernel uses (Initialize_LUT_pointers :228-250 with
@@ -244,6 +247,7 @@ struct Coder {
     const uint8_t *tab;  // LUT bytes
     const int32_t *slot_in;
     int32_t *slot_out;
+    uint32_t in_cap;  // decoder: words readable at slot_in (slot size, or the compact length)
     int lane, gl, g, msb;
     int top;  // highest stored bitplane (-1: none)
     uint32_t gmask, ltmask;
@@ -319,13 +323,13 @@ struct Coder {
         for (int q = 0; q < per; q += 4) {
             const uint32_t k = first + (uint32_t)(gl * per + q);
             uint32_t v0, v1, v2, v3;
-            if (k + 3 < (uint32_t)G::CAP) {
+            if (k + 3 < in_cap && p.offsets == nullptr) {
                 w.load4(slot_in + k, v0, v1, v2, v3);
-            } else {
-                v0 = k + 0 < (uint32_t)G::CAP ? (uint32_t)slot_in[k + 0] : 0xFFFFFFFFu;
-                v1 = k + 1 < (uint32_t)G::CAP ? (uint32_t)slot_in[k + 1] : 0xFFFFFFFFu;
-                v2 = k + 2 < (uint32_t)G::CAP ? (uint32_t)slot_in[k + 2] : 0xFFFFFFFFu;
-                v3 = k + 3 < (uint32_t)G::CAP ? (uint32_t)slot_in[k + 3] : 0xFFFFFFFFu;
+            } else {  // slot end, or the compact container (no 16-byte alignment)
+                v0 = k + 0 < in_cap ? (uint32_t)slot_in[k + 0] : 0xFFFFFFFFu;
+                v1 = k + 1 < in_cap ? (uint32_t)slot_in[k + 1] : 0xFFFFFFFFu;
+                v2 = k + 2 < in_cap ? (uint32_t)slot_in[k + 2] : 0xFFFFFFFFu;
+                v3 = k + 3 < in_cap ? (uint32_t)slot_in[k + 3] : 0xFFFFFFFFu;
             }
             const uint32_t r = k & (G::RING - 1);
             ring[r] = v0;
@@ -931,7 +935,15 @@ struct Coder {
             s.XNL = gl > 0 ? up : 0ull;
             s.XNR = gl < G::NL - 1 ? dn : 0ull;
         } else {
-            slot_in = p.in + (ok ? (size_t)cb * cap : 0);
+            if (p.offsets) {  // compact container; words past the codeblock read as the -1 fill
+                const long long o0 = ok ? p.offsets[cb] : 0, o1 = ok ? p.offsets[cb + 1] : 0;
+                slot_in = p.in + o0;
+                const long long n = o1 - o0;
+                in_cap = (uint32_t)(n < 0 ? 0 : (n > (long long)cap ? (long long)cap : n));
+            } else {
+                slot_in = p.in + (ok ? (size_t)cb * cap : 0);
+                in_cap = (uint32_t)cap;
+            }
             if (ok) {
                 ring_load(0u, G::RING);
                 s.ring_hi = G::RING;

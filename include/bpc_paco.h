@@ -104,6 +104,34 @@ int bpc_encode_device(const int *d_coeffs, int *d_stream, int X, int Y, const in
 int bpc_decode_device(const int *d_stream, int *d_coeffs, int X, int Y, const int *d_lut, int lut_n, int passes,
                       int levels, int cb_size, int *d_status, int *d_counts, int grid, void *stream);
 
+/* ---------------------------------------------------------------------------
+ * Batched persistent coding (no counterpart in the reference, which codes one
+ * image per call): many images of mixed size, DWT levels, pass count and
+ * codeblock size, one persistent kernel per (passes, codeblock size) class fed
+ * from a device work queue, the whole call captured in a CUDA graph.
+ * Output is the compact container: codeblock g (images in order, codeblocks in
+ * raster order) occupies compact[offsets[g] .. offsets[g+1]) = MSB word then
+ * its codewords; offsets has codeblocks + 1 entries.  The compact container
+ * needs at most bpc_batch_words() ints.
+ * ------------------------------------------------------------------------- */
+int bpc_batch_create(int n_images, const int *X, const int *Y, const int *levels, const int *passes,
+                     const int *cb_size, const int *const *d_luts, const int *lut_n, void **batch);
+long long bpc_batch_codeblocks(const void *batch);
+long long bpc_batch_words(const void *batch);
+int bpc_batch_encode(void *batch, const int *const *d_coeffs, int *d_compact, long long *d_offsets, int *d_status,
+                     void *stream);
+int bpc_batch_decode(void *batch, const int *d_compact, const long long *d_offsets, int *const *d_coeffs,
+                     int *d_status, void *stream);
+/* Schedule: CTAs per SM for the encoder (1..4) and decoder (1..7), codeblocks
+ * per work item, CUDA graph on/off.  bpc_batch_tune times the candidates on the
+ * given buffers and keeps the fastest. */
+int bpc_batch_set_schedule(void *batch, int ctas_per_sm_enc, int ctas_per_sm_dec, int cbs_per_item, int use_graph);
+int bpc_batch_get_schedule(const void *batch, int *ctas_per_sm_enc, int *ctas_per_sm_dec, int *cbs_per_item,
+                           int *use_graph);
+int bpc_batch_tune(void *batch, const int *const *d_coeffs, int *d_compact, long long *d_offsets, int *const *d_out,
+                   void *stream, double *best_us);
+int bpc_batch_destroy(void *batch);
+
 /* Number of ints of the loader array for a LUT folder's bitplane count. */
 int bpc_lut_entries(int passes, int levels, int max_bitplane);
 
