@@ -18,7 +18,7 @@ LIB_PATH = os.path.join(HERE, "libbpc_paco.so")
 
 CODE, DECODE = 0, 1
 OK = 0
-ERR_ARG, ERR_CUDA, ERR_FILE, ERR_PARSE, ERR_NOMEM = -1, -2, -3, -4, -5
+ERR_ARG, ERR_CUDA, ERR_FILE, ERR_PARSE, ERR_NOMEM, ERR_TOO_LARGE = -1, -2, -3, -4, -5, -6
 ST_SLOT_OVERFLOW, ST_BAD_STREAM, ST_INPUT_RANGE, ST_LUT_RANGE = 1, 2, 4, 8
 
 EXPORTS = ("CUDA_BPC", "load_LUTs", "bpc_set_mode", "bpc_get_mode", "bpc_last_status", "bpc_status_string",
@@ -273,3 +273,20 @@ def slots_to_compact(stream: np.ndarray, cb: int) -> list:
         n = int(np.count_nonzero(row[1:] != -1))
         out.append(row[:1 + n])
     return out
+
+
+def encode_compact_noalloc(coeffs, compact, offsets, lut: DeviceLut, cb: int = 64, status=None,
+                           cuda_stream: int | None = None) -> int:
+    """One-image encode into the compact container without allocating
+    (bpc_encode_compact_noalloc): for callers that may not allocate device
+    memory while they code.  Returns the C status (negative on error)."""
+    import torch
+    L = lib()
+    vp = ctypes.c_void_p
+    L.bpc_encode_compact_noalloc.argtypes = [vp, ctypes.c_int, ctypes.c_int, vp, ctypes.c_int, ctypes.c_int,
+                                             ctypes.c_int, ctypes.c_int, vp, vp, vp, vp]
+    L.bpc_encode_compact_noalloc.restype = ctypes.c_int
+    Y, X = coeffs.shape
+    s = torch.cuda.current_stream().cuda_stream if cuda_stream is None else cuda_stream
+    return L.bpc_encode_compact_noalloc(_ptr(coeffs), X, Y, vp(lut.ptr), lut.n, lut.passes, lut.levels, cb,
+                                        _ptr(compact), _ptr(offsets), vp(_ptr(status)), vp(s))

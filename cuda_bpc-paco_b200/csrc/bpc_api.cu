@@ -135,6 +135,7 @@ const char *bpc_status_string(int st) {
         case BPC_ERR_FILE: return "cannot open LUT file";
         case BPC_ERR_PARSE: return "malformed LUT file";
         case BPC_ERR_NOMEM: return "out of memory";
+        case BPC_ERR_TOO_LARGE: return "image larger than the no-allocation entry point's fixed scratch";
         default: break;
     }
     if (st > 0) {

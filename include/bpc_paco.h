@@ -36,6 +36,7 @@ enum { BPC_CODE = 0, BPC_DECODE = 1 };
 #define BPC_ERR_FILE (-3)
 #define BPC_ERR_PARSE (-4)
 #define BPC_ERR_NOMEM (-5)
+#define BPC_ERR_TOO_LARGE (-6) /* image larger than bpc_encode_compact_noalloc's fixed scratch */
 #define BPC_ST_SLOT_OVERFLOW 1
 #define BPC_ST_BAD_STREAM 2
 #define BPC_ST_INPUT_RANGE 4
@@ -131,6 +132,22 @@ int bpc_batch_get_schedule(const void *batch, int *ctas_per_sm_enc, int *ctas_pe
 int bpc_batch_tune(void *batch, const int *const *d_coeffs, int *d_compact, long long *d_offsets, int *const *d_out,
                    void *stream, double *best_us);
 int bpc_batch_destroy(void *batch);
+
+/* One-image encode into the compact container that allocates no memory.  No
+ * counterpart in the reference.  For callers that may not call cudaMalloc while
+ * they code: an application whose device memory is already handed to its own
+ * pool, a latency-critical stream an allocation would stall, a plugin its host
+ * only gives device pointers.  The scratch this encode needs (slot stream,
+ * per-codeblock counts and sizes, prefix-scan workspace) lives in one fixed
+ * 16.1 MiB device array inside the library, held by every GPU that loads this
+ * code until the process exits.  Limit: X*Y <= 2048*2048 coefficients, else
+ * BPC_ERR_TOO_LARGE.  Output as bpc_batch_encode for a one-image batch:
+ * d_compact (at most X*Y ints) and d_offsets (codeblocks + 1 entries).  The
+ * first call on each device looks the array's device address up; make that
+ * call before any stream capture.  All calls share the array: calls that
+ * overlap on the GPU race, so serialise them. */
+int bpc_encode_compact_noalloc(const int *d_coeffs, int X, int Y, const int *d_lut, int lut_n, int passes, int levels,
+                               int cb_size, int *d_compact, long long *d_offsets, int *d_status, void *stream);
 
 /* Number of ints of the loader array for a LUT folder's bitplane count. */
 int bpc_lut_entries(int passes, int levels, int max_bitplane);
