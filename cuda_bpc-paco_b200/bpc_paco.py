@@ -290,3 +290,18 @@ def encode_compact_noalloc(coeffs, compact, offsets, lut: DeviceLut, cb: int = 6
     s = torch.cuda.current_stream().cuda_stream if cuda_stream is None else cuda_stream
     return L.bpc_encode_compact_noalloc(_ptr(coeffs), X, Y, vp(lut.ptr), lut.n, lut.passes, lut.levels, cb,
                                         _ptr(compact), _ptr(offsets), vp(_ptr(status)), vp(s))
+
+
+def dwt53(data, levels: int, inverse: bool = False, tmp=None, cuda_stream: int | None = None) -> None:
+    """In-place reversible 5/3 DWT of a torch int32 (Y x X) tensor on the GPU
+    (bpc_dwt53_forward / _inverse)."""
+    import torch
+    L = lib()
+    vp = ctypes.c_void_p
+    f = L.bpc_dwt53_inverse if inverse else L.bpc_dwt53_forward
+    f.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp, vp]
+    f.restype = ctypes.c_int
+    Y, X = data.shape
+    t = torch.empty_like(data) if tmp is None else tmp
+    s = torch.cuda.current_stream().cuda_stream if cuda_stream is None else cuda_stream
+    _check(f(vp(data.data_ptr()), X, Y, levels, vp(t.data_ptr()), vp(s)), "bpc_dwt53")

@@ -143,3 +143,45 @@ def laplacian_coefficients(side: int, levels: int, seed: int, max_plane: int = 1
     out[:h, :h] = np.rint(rng.laplace(0.0, 2.0 ** (levels + 3), size=(h, h)))
     lim = (1 << (max_plane + 1)) - 1
     return np.clip(out, -lim, lim).astype(np.int32)
+
+
+def make_image_gpu(side: int, seed: int, amp: float = 20.0, nrect: int = 30, device="cuda"):
+    """The same kind of image as make_image, generated with torch on the GPU
+    (its own RNG stream, so the pixels differ from make_image's): 4
+    low-frequency sinusoids + blurred uniform noise + constant rectangles,
+    clipped to [0, 255].  Returns an int32 tensor."""
+    import torch
+    g = torch.Generator(device="cpu").manual_seed(seed)
+    H = W = side
+    y = torch.arange(H, device=device, dtype=torch.float32)[:, None]
+    x = torch.arange(W, device=device, dtype=torch.float32)[None, :]
+    img = torch.full((H, W), 128.0, device=device)
+    for _ in range(4):
+        a, fx, fy, ph = (torch.rand(4, generator=g) * torch.tensor([25.0, 3.7, 3.7, 6.2832]) +
+                         torch.tensor([10.0, 0.3, 0.3, 0.0])).tolist()
+        img += a * torch.sin(2 * np.pi * (fx / W * x + fy / H * y) + ph)
+    gg = torch.Generator(device=device).manual_seed(seed)
+    noise = (torch.rand((1, 1, H, W), generator=gg, device=device) * 2 - 1) * amp
+    k = torch.from_numpy(_gauss_kernel(1.5)).to(device)
+    r = k.numel() // 2
+    noise = torch.nn.functional.conv2d(torch.nn.functional.pad(noise, (r, r, 0, 0), mode="reflect"),
+                                       k.view(1, 1, 1, -1))
+    noise = torch.nn.functional.conv2d(torch.nn.functional.pad(noise, (0, 0, r, r), mode="reflect"),
+                                       k.view(1, 1, -1, 1))
+    img += noise[0, 0]
+    rr = torch.rand((nrect, 5), generator=g).tolist()
+    for (u0, u1, u2, u3, u4) in rr:
+        w = int(max(2, W // 64) + u0 * (max(3, W // 5) - max(2, W // 64)))
+        h = int(max(2, H // 64) + u1 * (max(3, H // 5) - max(2, H // 64)))
+        x0 = int(u2 * (W - w))
+        y0 = int(u3 * (H - h))
+        img[y0:y0 + h, x0:x0 + w] += -80.0 + 160.0 * u4
+    return torch.clamp(torch.round(img), 0, 255).to(torch.int32)
+
+
+def synthetic_coefficients_gpu(side: int, levels: int, seed: int, amp: float = 20.0, nrect: int = 30, tmp=None):
+    """make_image_gpu -> level shift -> 5/3 DWT on the GPU (bpc_dwt53_forward)."""
+    import bpc_paco
+    img = make_image_gpu(side, seed, amp, nrect) - 128
+    bpc_paco.dwt53(img, levels, tmp=tmp)
+    return img

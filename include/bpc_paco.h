@@ -149,6 +149,14 @@ int bpc_batch_destroy(void *batch);
 int bpc_encode_compact_noalloc(const int *d_coeffs, int X, int Y, const int *d_lut, int lut_n, int passes, int levels,
                                int cb_size, int *d_compact, long long *d_offsets, int *d_status, void *stream);
 
+/* Reversible CDF 5/3 lifting DWT (JPEG 2000 integer filter) on the GPU, in
+ * place on an X x Y int32 raster, `levels` levels, Mallat layout (LL top-left,
+ * HL top-right, LH bottom-left, HH bottom-right) -- the input format of the
+ * coder.  No counterpart in the reference, which takes pre-transformed data.
+ * d_tmp: device scratch of X*Y ints.  X and Y must be multiples of 2^levels. */
+int bpc_dwt53_forward(int *d_data, int X, int Y, int levels, int *d_tmp, void *stream);
+int bpc_dwt53_inverse(int *d_data, int X, int Y, int levels, int *d_tmp, void *stream);
+
 /* Number of ints of the loader array for a LUT folder's bitplane count. */
 int bpc_lut_entries(int passes, int levels, int max_bitplane);
 
