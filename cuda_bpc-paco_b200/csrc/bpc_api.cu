@@ -28,6 +28,11 @@ struct DropInState {
     // device buffers reused across CUDA_BPC calls (grow only)
     int *d_a = nullptr, *d_b = nullptr, *d_status = nullptr;
     size_t cap = 0;
+    // host-buffer calls run bands of codeblock rows on these streams so that
+    // the copies in both directions overlap the kernels
+    static constexpr int kStreams = 3;
+    cudaStream_t streams[kStreams] = {};
+    cudaEvent_t done[kStreams] = {};
 };
 
 DropInState &state() {
@@ -67,14 +72,20 @@ int fill_params(bpc::Params &p, const int *in, int *out, int X, int Y, const int
     p.status = d_status;
     p.counts = d_counts;
     p.offsets = nullptr;
+    p.cb_begin = 0;
+    p.cb_end = p.ncb;
     return BPC_OK;
 }
 
 int code_device(bool enc, const int *in, int *out, int X, int Y, const int *d_lut, int lut_n, int passes, int levels,
-                int cb, int *d_status, int *d_counts, int grid, void *stream) {
+                int cb, int *d_status, int *d_counts, int grid, void *stream, int cb_begin = 0, int cb_end = -1) {
     bpc::Params p;
     const int rc = fill_params(p, in, out, X, Y, d_lut, lut_n, passes, levels, cb, d_status, d_counts);
     if (rc) return rc;
+    if (cb_end >= 0) {
+        p.cb_begin = cb_begin;
+        p.cb_end = cb_end;
+    }
     const cudaError_t e = bpc::launch_code(enc, passes, cb, p, grid, (cudaStream_t)stream);
     if (e != cudaSuccess) {
         std::fprintf(stderr, "bpc: kernel launch failed: %s\n", cudaGetErrorString(e));
@@ -109,15 +120,42 @@ int code_host_locked(DropInState &s, int direction, int *hdata, int X, int Y, co
         s.cap = n;
     }
     if (!s.d_status) CUDA_TRY(cudaMalloc((void **)&s.d_status, sizeof(int)));
-    CUDA_TRY(cudaMemsetAsync(s.d_status, 0, sizeof(int), 0));
-    CUDA_TRY(cudaMemcpyAsync(s.d_a, hdata, n * sizeof(int), cudaMemcpyHostToDevice, 0));
-    int rc = code_device(direction == BPC_CODE, s.d_a, s.d_b, X, Y, d_lut, lut_n, passes, levels, cb, s.d_status,
-                         nullptr, 0, nullptr);
-    if (rc) return rc;
-    CUDA_TRY(cudaMemcpyAsync(hdata, s.d_b, n * sizeof(int), cudaMemcpyDeviceToHost, 0));
+    if (!s.streams[0])
+        for (int k = 0; k < DropInState::kStreams; k++) {
+            CUDA_TRY(cudaStreamCreateWithFlags(&s.streams[k], cudaStreamNonBlocking));
+            CUDA_TRY(cudaEventCreateWithFlags(&s.done[k], cudaEventDisableTiming));
+        }
+    CUDA_TRY(cudaMemsetAsync(s.d_status, 0, sizeof(int), s.streams[0]));
+    CUDA_TRY(cudaEventRecord(s.done[0], s.streams[0]));
+    for (int k = 1; k < DropInState::kStreams; k++) CUDA_TRY(cudaStreamWaitEvent(s.streams[k], s.done[0], 0));
+    // bands of codeblock rows: the input rows and the output slots of a band
+    // are contiguous in both layouts (coefficients row-major, slots in raster
+    // order of codeblocks)
+    const int ncbx = X / cb, rows = Y / cb;
+    // at least ~1024 codeblocks per band so that each band's kernel still fills the GPU
+    const long long ncb = (long long)ncbx * rows;
+    int nband = (int)(ncb / 1024);
+    nband = nband < 1 ? 1 : (nband > 8 ? 8 : nband);
+    if (nband > rows) nband = rows;
+    const size_t row_words = (size_t)X * (size_t)cb;  // one codeblock row, either layout
+    for (int k = 0; k < nband; k++) {
+        const int r0 = (int)((long long)rows * k / nband), r1 = (int)((long long)rows * (k + 1) / nband);
+        if (r1 <= r0) continue;
+        cudaStream_t st = s.streams[k % DropInState::kStreams];
+        const size_t off = (size_t)r0 * row_words, cnt = (size_t)(r1 - r0) * row_words;
+        CUDA_TRY(cudaMemcpyAsync(s.d_a + off, hdata + off, cnt * sizeof(int), cudaMemcpyHostToDevice, st));
+        const int rc = code_device(direction == BPC_CODE, s.d_a, s.d_b, X, Y, d_lut, lut_n, passes, levels, cb,
+                                   s.d_status, nullptr, 0, st, r0 * ncbx, r1 * ncbx);
+        if (rc) return rc;
+        CUDA_TRY(cudaMemcpyAsync(hdata + off, s.d_b + off, cnt * sizeof(int), cudaMemcpyDeviceToHost, st));
+    }
+    for (int k = 1; k < DropInState::kStreams; k++) {
+        CUDA_TRY(cudaEventRecord(s.done[k], s.streams[k]));
+        CUDA_TRY(cudaStreamWaitEvent(s.streams[0], s.done[k], 0));
+    }
     int st = 0;
-    CUDA_TRY(cudaMemcpyAsync(&st, s.d_status, sizeof(int), cudaMemcpyDeviceToHost, 0));
-    CUDA_TRY(cudaStreamSynchronize(0));
+    CUDA_TRY(cudaMemcpyAsync(&st, s.d_status, sizeof(int), cudaMemcpyDeviceToHost, s.streams[0]));
+    CUDA_TRY(cudaStreamSynchronize(s.streams[0]));
     return st;
 }
 

@@ -125,6 +125,8 @@ __global__ void __launch_bounds__(kWarps * 32, ENC ? kMinCtasEnc : kMinCtasDec)
         p.status = status;
         p.counts = counts ? counts + im.cb_base : nullptr;
         p.offsets = offsets ? offsets + im.cb_base : nullptr;
+        p.cb_begin = 0;
+        p.cb_end = im.ncb;
         for (int k = 0; k < item.n; k += G::NG) {
             Coder<PASSES, CBS, ENC, GpuWarpB> cd(w, p, ring, im.tab, planes, ev_key, ev_val);
             cd.run(item.cb0 + k);

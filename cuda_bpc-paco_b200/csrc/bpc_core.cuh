@@ -59,6 +59,7 @@ struct Params {
     // decoder input in the compact container: codeblock k's words (MSB and
     // codewords) are in[offsets[k] .. offsets[k+1]); null = slot layout
     const long long *offsets;
+    int cb_begin, cb_end;  // codeblocks [cb_begin, cb_end) of the image are coded by this launch
 };
 
 // LUT offsets the reference kernel uses (Initialize_LUT_pointers :228-250 with
@@ -858,7 +859,7 @@ struct Coder {
     BPC_FI void run(int cb_first) {
         const int grp = lane / G::NL;
         const int cb = cb_first + grp;
-        const bool ok = cb < p.ncb;
+        const bool ok = cb < p.cb_end;
         const int cbx = ok ? cb % p.ncbx : 0, cby = ok ? cb / p.ncbx : 0;
         const int x = cbx * CBS + 2 * gl, y0 = cby * CBS;
         // Find_Subband :84-111, per lane (x of the lane, y of the block top)

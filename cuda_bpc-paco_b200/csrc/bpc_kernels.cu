@@ -69,7 +69,7 @@ __global__ void __launch_bounds__(kWarps * 32, ENC ? kMinCtasEnc : kMinCtasDec) 
     uint8_t ev_key[ENC ? 256 : 1];
     uint32_t ev_val[ENC ? 256 : 1];
     const int stride = (int)gridDim.x * kWarps * G::NG;
-    for (int base = ((int)blockIdx.x * kWarps + warp) * G::NG; base < p.ncb; base += stride) {
+    for (int base = p.cb_begin + ((int)blockIdx.x * kWarps + warp) * G::NG; base < p.cb_end; base += stride) {
         Coder<PASSES, CBS, ENC, GpuWarp> cd(w, p, ring, tab, planes, ev_key, ev_val);
         cd.run(base);
     }
@@ -87,7 +87,7 @@ static cudaError_t launch_t(const Params &p, int grid, cudaStream_t st) {
     const size_t sm = smem_bytes<PASSES, CBS, ENC>(p);
     cudaError_t e = cudaFuncSetAttribute(k_bpc<PASSES, CBS, ENC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return e;
-    const int warps_needed = (p.ncb + G::NG - 1) / G::NG;
+    const int warps_needed = (p.cb_end - p.cb_begin + G::NG - 1) / G::NG;
     const int full = (warps_needed + kWarps - 1) / kWarps;
     if (grid <= 0 || grid > full) grid = full;
     if (grid < 1) grid = 1;
@@ -96,7 +96,7 @@ static cudaError_t launch_t(const Params &p, int grid, cudaStream_t st) {
 }
 
 cudaError_t launch_code(bool enc, int passes, int cbs, const Params &p, int grid, cudaStream_t st) {
-    if (p.ncb <= 0) return cudaSuccess;
+    if (p.cb_end <= p.cb_begin) return cudaSuccess;
     if (enc) {
         if (passes == 2) return cbs == 64 ? launch_t<2, 64, true>(p, grid, st) : launch_t<2, 32, true>(p, grid, st);
         return cbs == 64 ? launch_t<3, 64, true>(p, grid, st) : launch_t<3, 32, true>(p, grid, st);

@@ -146,6 +146,8 @@ extern "C" int bpc_encode_compact_noalloc(const int *d_coeffs, int X, int Y, con
     p.status = d_status;
     p.counts = counts;
     p.offsets = nullptr;
+    p.cb_begin = 0;
+    p.cb_end = p.ncb;
     cudaError_t e = bpc::launch_code(true, passes, cb_size, p, 0, st);
     const long long ncb = p.ncb, cap = (long long)cb_size * cb_size;
     if (e == cudaSuccess) {
