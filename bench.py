@@ -38,7 +38,9 @@ CONFIGS = {
     # name: side, levels, passes, cb, amp, nrect
     "cfg1": dict(side=2048, levels=5, passes=2, cb=64, amp=20.0, nrect=30),
     "cfg2": dict(side=4096, levels=5, passes=3, cb=64, amp=40.0, nrect=60),
-    "cfg5": dict(side=16384, levels=5, passes=3, cb=64, amp=80.0, nrect=400),
+    "cfg5": dict(side=16384, levels=5, passes=3, cb=64, amp=80.0, nrect=400, gpu_input=True),
+    # cfg5's second input: i.i.d. Laplacian coefficients, every codeblock coding 16 planes
+    "cfg5l": dict(side=16384, levels=5, passes=3, cb=64, laplacian=True, gpu_input=True),
 }
 METRIC = "encode/decode Gcoeff/s (bit-exact)"
 # DRAM read + write bytes of one launch of the dominant kernel (the decoder),
@@ -47,8 +49,9 @@ NCU_TRAFFIC = {"cfg2": 14.621440e6 + 19.690496e6}
 
 
 def workload_name(c):
-    return (f"{c['side']}x{c['side']} synthetic image, {c['levels']}-level CDF 5/3 DWT, "
-            f"{c['cb']}x{c['cb']} codeblocks, {c['passes']}-pass encode+decode")
+    src = ("i.i.d. Laplacian coefficients (scale 2^(level+3), 16 planes per codeblock)" if c.get("laplacian")
+           else f"synthetic image, {c['levels']}-level CDF 5/3 DWT")
+    return f"{c['side']}x{c['side']} {src}, {c['cb']}x{c['cb']} codeblocks, {c['passes']}-pass encode+decode"
 
 
 def load_peaks():
@@ -114,6 +117,23 @@ def dist_info():
     return rank, world, local
 
 
+def rank_seed(rank: int) -> int:
+    """Each rank codes its own image (seed 1 + rank): images are independent,
+    so the work shards by image with no exchange between ranks."""
+    return 1 + rank
+
+
+def max_over_ranks(x: float, device=None) -> float:
+    """The slowest rank's time (the job's time); x itself when not distributed."""
+    import torch
+    import torch.distributed as tdist
+    if not (tdist.is_available() and tdist.is_initialized()) or tdist.get_world_size() == 1:
+        return x
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def cpu_baseline(img, lut_np, c, budget_s=12.0):
     """Oracle (CPU restatement) encode + decode on all host cores over a
     bounded prefix of the codeblocks."""
@@ -137,7 +157,14 @@ def cpu_baseline(img, lut_np, c, budget_s=12.0):
 
 
 def make_input(c, seed):
+    """Seeded coefficients of the configuration as a host int32 array (the
+    HBM-scale configurations are generated on the GPU and copied back)."""
     import bpc_synth
+    if c.get("laplacian"):
+        return bpc_synth.laplacian_coefficients_gpu(c["side"], c["levels"], seed, cb=c["cb"]).cpu().numpy()
+    if c.get("gpu_input"):
+        return bpc_synth.synthetic_coefficients_gpu(c["side"], c["levels"], seed, amp=c["amp"],
+                                                    nrect=c["nrect"]).cpu().numpy()
     return bpc_synth.synthetic_coefficients(c["side"], c["levels"], seed, amp=c["amp"], nrect=c["nrect"])
 
 
@@ -194,7 +221,6 @@ def run_batched(args):
     import torch
     import bpc_paco as bpc
     import bpc_synth
-    import oracle
 
     specs = cfg3_specs(args.images)
     luts = {2: os.path.join(LUT_DIR, "2_coding_pass"), 3: os.path.join(LUT_DIR, "3_coding_pass")}
@@ -236,24 +262,32 @@ def run_batched(args):
         batched_step()
     torch.cuda.synchronize()
     status = st.item()
-    # bit-exactness: lossless where no codeblock overflowed; sampled codeblocks vs the oracle
+    # bit-exactness: lossless where no codeblock overflowed; every image's
+    # container equals the plain kernel's slot stream of the same image (the
+    # plain kernel is the one the parity tests hold bit-exact to the oracle)
     lossless = sum(int(torch.equal(o, i)) for o, i in zip(out, d_in))
     offs_h = offs.cpu().numpy()
     checked = 0
     base = 0
-    rng = np.random.default_rng(7)
+    lut_chk = {}
+    slot_chk = torch.empty(8192 * 8192, dtype=torch.int32, device="cuda")
     for k, (X, Y, lv, ps, cb) in enumerate(specs):
         ncb = (X // cb) * (Y // cb)
-        if k % 48 == 0:
-            img = d_in[k].cpu().numpy()
-            lut_np = oracle.load_luts(luts[ps], ps, lv)
-            for g in rng.choice(ncb, size=min(ncb, 24), replace=False):
-                s = oracle.encode(img, lut_np, ps, lv, cb, cb_range=(int(g), int(g) + 1))
-                want = bpc.slots_to_compact(s, cb)[int(g)]
-                got = compact[offs_h[base + g]:offs_h[base + g + 1]].cpu().numpy()
-                assert np.array_equal(got, want), f"image {k} codeblock {g} differs from the oracle"
-                checked += 1
+        if (ps, lv) not in lut_chk:
+            lut_chk[(ps, lv)] = bpc.DeviceLut(luts[ps], ps, lv)
+        sv = slot_chk[:X * Y]
+        bpc.encode_device(d_in[k], sv, lut_chk[(ps, lv)], cb)
+        slots = sv.view(ncb, cb * cb)
+        sizes = torch.clamp((slots[:, 1:] != -1).sum(1) + 1, max=cb * cb)
+        assert torch.equal(offs[base + 1:base + ncb + 1] - offs[base:base + ncb], sizes), f"image {k}: sizes differ"
+        want = slots[torch.arange(cb * cb, device="cuda")[None, :] < sizes[:, None]]
+        got = compact[int(offs_h[base]):int(offs_h[base + ncb])]
+        assert torch.equal(got, want), f"image {k}: container differs from the plain stream"
+        checked += ncb
         base += ncb
+    for l in lut_chk.values():
+        l.close()
+    del slot_chk
     times = []
     torch.cuda.synchronize()
     with ClockSampler(0) as clk:
@@ -303,7 +337,7 @@ def run_batched(args):
         "encode_gcoeffs": total / te / 1e9, "decode_gcoeffs": total / td / 1e9,
         "plain_per_image_gcoeffs": 2 * total / tp / 1e9, "batched_over_plain": tp / (te + td),
         "compact_words": words, "compression": 4.0 * total / (4.0 * words),
-        "status": status, "images_lossless": lossless, "codeblocks_checked_vs_oracle": checked,
+        "status": status, "images_lossless": lossless, "codeblocks_checked_vs_plain_stream": checked,
         "gpu_launches": "4 persistent kernels + scan + gather per encode, 4 per decode (one CUDA graph each)",
         "roofline": {"bound": "hbm", "achieved": alg / max(te, td) / 1e9, "peak": peak, "unit": "GB/s",
                      "frac": alg / max(te, td) / 1e9 / peak, "traffic": None, "peak_source": peak_kind},
@@ -312,6 +346,164 @@ def run_batched(args):
     for d in lut_dev.values():
         d.close()
     b.close()
+    print(json.dumps(line))
+
+
+def cfg4_specs(n=20000, seed=4):
+    """n requests: 60 % encode / 40 % decode; side log-uniform in [2048, 8192]
+    rounded to a multiple of 1024; DWT levels 3..6, 2 or 3 passes, 64x64
+    codeblocks for 70 % (else 32x32), as in cfg3."""
+    rng = np.random.default_rng(seed)
+    side = np.exp(rng.uniform(np.log(2048), np.log(8192), n))
+    side = np.clip(np.round(side / 1024) * 1024, 2048, 8192).astype(int)
+    out = []
+    for k in range(n):
+        out.append((bpc_dir(rng.random() < 0.6), int(side[k]), int(rng.integers(3, 7)), int(rng.choice([2, 3])),
+                    64 if rng.random() < 0.7 else 32))
+    return out
+
+
+def bpc_dir(encode: bool) -> int:
+    return 0 if encode else 1  # BPC_CODE / BPC_DECODE
+
+
+def run_served(args):
+    """cfg4: a Poisson stream of encode/decode requests through the request
+    server, at saturation and at 20/50/80/100 % of the saturated rate, against
+    the plain form (the same server with one request on the GPU at a time,
+    i.e. one launch per request back to back).  Every output is compared on
+    the GPU with the one-request result of the same input."""
+    import collections
+
+    import torch
+    import bpc_paco as bpc
+    import bpc_synth
+
+    reqs = cfg4_specs(args.requests)
+    luts_dir = {2: os.path.join(LUT_DIR, "2_coding_pass"), 3: os.path.join(LUT_DIR, "3_coding_pass")}
+    combos = sorted({(sd, lv, ps, cb) for (_, sd, lv, ps, cb) in reqs})
+    lut_dev = {(ps, lv): bpc.DeviceLut(luts_dir[ps], ps, lv) for (_, lv, ps, _) in combos}
+    # resident inputs: per combination one coefficient image, its stream (the
+    # input of decode requests and the expected encode output) and, where the
+    # stream is lossy (a codeblock overflowed its slot), the expected decode
+    tmp = torch.empty(8192 * 8192, dtype=torch.int32, device="cuda")
+    coef, strm, decd, cstat = {}, {}, {}, {}
+    pool_bytes = 0
+    for k, key in enumerate(combos):
+        sd, lv, ps, cb = key
+        x = bpc_synth.synthetic_coefficients_gpu(sd, lv, 4000 + k, amp=30.0, nrect=max(30, sd // 64),
+                                                 tmp=tmp[:sd * sd].view(sd, sd))
+        st = torch.zeros(1, dtype=torch.int32, device="cuda")
+        s_ = torch.empty_like(x)
+        bpc.encode_device(x, s_, lut_dev[(ps, lv)], cb, st)
+        d_ = torch.empty_like(x)
+        bpc.decode_device(s_, d_, lut_dev[(ps, lv)], cb, st)
+        torch.cuda.synchronize()
+        coef[key], strm[key], cstat[key] = x.view(-1), s_.view(-1), st.item()
+        pool_bytes += 8 * x.numel()
+        if not torch.equal(d_, x):
+            decd[key] = d_.view(-1)
+            pool_bytes += 4 * x.numel()
+        else:
+            del d_
+    del tmp
+    torch.cuda.synchronize()
+    budget = int(args.budget_gb * 1e9) - pool_bytes  # resident inputs count against the 120 GB
+    vs = torch.cuda.Stream()
+    bad = torch.zeros(1, dtype=torch.int64, device="cuda")
+    ncoef = np.array([sd * sd for (_, sd, _, _, _) in reqs], np.float64)
+
+    def serve(srv, ids, rlist, rate, seed):
+        n = len(rlist)
+        if rate is None:
+            arr = np.zeros(n)
+        else:
+            arr = np.cumsum(np.random.default_rng(seed).exponential(1.0 / rate, n))
+        lat = np.zeros(n)
+        stat = np.zeros(n, np.int64)
+        tick = {}
+        pending = collections.deque()
+        i = done = 0
+        t_last = 0.0
+        t0 = time.perf_counter()
+        while done < n:
+            now = time.perf_counter() - t0
+            while i < n and arr[i] <= now:
+                d, sd, lv, ps, cb = rlist[i]
+                key = (sd, lv, ps, cb)
+                src = coef[key] if d == 0 else strm[key]
+                t = srv.submit(d, src, ids[(ps, lv)], cb, shape=(sd, sd))
+                assert t >= 0, t
+                tick[t] = i
+                i += 1
+            wait = 1000 if i >= n else int(max(0.0, min(1e-3, arr[i] - (time.perf_counter() - t0))) * 1e6)
+            for t, ptr, us, st in srv.poll(256, wait):
+                k = tick.pop(t)
+                assert st >= 0 and ptr, f"request {k} failed: {st}"
+                lat[k], stat[k] = us, st
+                done += 1
+                t_last = time.perf_counter() - t0
+                d, sd, lv, ps, cb = rlist[k]
+                key = (sd, lv, ps, cb)
+                want = strm[key] if d == 0 else decd.get(key, coef[key])
+                view = bpc.as_tensor(ptr, sd * sd)
+                with torch.cuda.stream(vs):
+                    bad.add_(torch.ne(view, want).any())
+                    ev = torch.cuda.Event()
+                    ev.record(vs)
+                pending.append((ev, ptr))
+            while pending and pending[0][0].query():
+                srv.release(pending.popleft()[1])
+        vs.synchronize()
+        while pending:
+            srv.release(pending.popleft()[1])
+        return lat, stat, t_last
+
+    def summary(lat, stat, span):
+        small = np.array([r[1] == 2048 for r in reqs])
+        q = lambda a, p: float(np.percentile(a, p)) / 1e3
+        return {"requests": len(reqs), "req_per_s": len(reqs) / span, "gcoeffs": float(ncoef.sum()) / span / 1e9,
+                "p50_ms": q(lat, 50), "p99_ms": q(lat, 99), "p99_9_ms": q(lat, 99.9),
+                "p50_ms_2048": q(lat[small], 50), "p99_ms_2048": q(lat[small], 99),
+                "requests_with_status": int((stat != 0).sum())}
+
+    result = {}
+    with ClockSampler(0) as clk:
+        for name, inflight in (("server", args.in_flight), ("plain", 1)):
+            srv = bpc.Server(budget, inflight)
+            ids = {key: srv.register_lut(l) for key, l in lut_dev.items()}
+            # warm-up: every combination once, both directions
+            warm = [(d, sd, lv, ps, cb) for (sd, lv, ps, cb) in combos for d in (0, 1)]
+            serve(srv, ids, warm, None, 0)
+            lat, stat, span = serve(srv, ids, reqs, None, 1)
+            out = {"saturated": summary(lat, stat, span)}
+            rate = len(reqs) / span
+            loads = args.loads if name == "server" else [0.8]
+            for f in loads:
+                lat, stat, span = serve(srv, ids, reqs, f * rate, 10 + int(100 * f))
+                out[f"load_{int(round(100 * f))}"] = dict(summary(lat, stat, span), offered_req_per_s=f * rate)
+            srv.close()
+            result[name] = out
+    torch.cuda.synchronize()
+    n_bad = int(bad.item())
+    sat, plain = result["server"]["saturated"], result["plain"]["saturated"]
+    line = {
+        "metric": "served requests: Gcoeff/s and p50/p99 latency (bit-exact)", "value": sat["gcoeffs"],
+        "unit": "Gcoeff/s", "n_gpus": 1, "steps": len(reqs), "warmup": 2 * len(combos), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic (GPU generator + GPU 5/3 DWT)",
+        "config": {"workload": f"cfg4: {len(reqs)} Poisson requests, 60/40 encode/decode, sides 2048-8192 "
+                               f"log-uniform (multiples of 1024), levels 3-6, 2/3 passes, 64x64 (70%) / 32x32",
+                   "budget_gb": args.budget_gb, "resident_inputs_gb": pool_bytes / 1e9,
+                   "max_in_flight": args.in_flight, "combinations": len(combos), "l2": "inputs >> L2"},
+        "server": result["server"], "plain": result["plain"],
+        "server_over_plain_saturated": sat["req_per_s"] / plain["req_per_s"],
+        "outputs_compared": len(reqs) * (len(args.loads) + 3), "outputs_differing": n_bad,
+        "combinations_with_status": int(sum(1 for v in cstat.values() if v)),
+        "gpu_launches": "1 coder launch + status memset/copy per request",
+        "clocks": clk.summary(),
+    }
+    for l in lut_dev.values():
+        l.close()
     print(json.dumps(line))
 
 
@@ -328,7 +520,7 @@ def run_ours(args, c):
         tdist.init_process_group("nccl", timeout=timedelta(seconds=120))
     dev = torch.device("cuda", local if dist else 0)
     torch.cuda.set_device(dev)
-    img = make_input(c, 1 + rank)
+    img = make_input(c, rank_seed(rank))
     X = Y = c["side"]
     N = X * Y
     passes, levels, cb = c["passes"], c["levels"], c["cb"]
@@ -375,10 +567,7 @@ def run_ours(args, c):
     te = sum(a.elapsed_time(b) for a, b, _, _ in times) / 1e3
     td = sum(c2.elapsed_time(d) for _, _, c2, d in times) / 1e3
     t_step = (te + td) / args.steps
-    if dist:
-        t = torch.tensor([t_step], dtype=torch.float64, device=dev)
-        tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
-        t_step = float(t.item())
+    t_step = max_over_ranks(t_step, dev)
     value = 2 * N * world / t_step / 1e9
 
     if args.no_e2e:
@@ -413,10 +602,7 @@ def run_ours(args, c):
             e2e_t.append((t1 - t0) + (t3 - t2))
     assert np.array_equal(hn.reshape(Y, X), img), "host-path decode differs"
     e2e_step = float(np.mean(e2e_t))
-    if dist:
-        t = torch.tensor([e2e_step], dtype=torch.float64, device=dev)
-        tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
-        e2e_step = float(t.item())
+    e2e_step = max_over_ranks(e2e_step, dev)
     e2e = 2 * N * world / e2e_step / 1e9
 
     peak, peak_kind = load_peaks()
@@ -456,14 +642,18 @@ def main():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="cfg2", choices=sorted(CONFIGS) + ["cfg3"])
+    ap.add_argument("--config", default="cfg2", choices=sorted(CONFIGS) + ["cfg3", "cfg4"])
     ap.add_argument("--images", type=int, default=192, help="cfg3: images per batch")
+    ap.add_argument("--requests", type=int, default=20000, help="cfg4: requests per load level")
+    ap.add_argument("--loads", type=float, nargs="+", default=[0.2, 0.5, 0.8, 1.0], help="cfg4: offered loads")
+    ap.add_argument("--in-flight", type=int, default=8, help="cfg4: requests on the GPU at once")
+    ap.add_argument("--budget-gb", type=float, default=120.0, help="cfg4: HBM admission budget")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="kernel timing only (profiling runs)")
     args = ap.parse_args()
-    if args.config == "cfg3":
+    if args.config in ("cfg3", "cfg4"):
         if args.impl == "ours":
-            run_batched(args)
+            (run_batched if args.config == "cfg3" else run_served)(args)
             return
         c = CONFIGS["cfg2"]
     else:

@@ -18,7 +18,7 @@ LIB_PATH = os.path.join(HERE, "libbpc_paco.so")
 
 CODE, DECODE = 0, 1
 OK = 0
-ERR_ARG, ERR_CUDA, ERR_FILE, ERR_PARSE, ERR_NOMEM, ERR_TOO_LARGE = -1, -2, -3, -4, -5, -6
+ERR_ARG, ERR_CUDA, ERR_FILE, ERR_PARSE, ERR_NOMEM, ERR_TOO_LARGE, ERR_CANCELLED = -1, -2, -3, -4, -5, -6, -7
 ST_SLOT_OVERFLOW, ST_BAD_STREAM, ST_INPUT_RANGE, ST_LUT_RANGE = 1, 2, 4, 8
 
 EXPORTS = ("CUDA_BPC", "load_LUTs", "bpc_set_mode", "bpc_get_mode", "bpc_last_status", "bpc_status_string",
@@ -305,3 +305,96 @@ def dwt53(data, levels: int, inverse: bool = False, tmp=None, cuda_stream: int |
     t = torch.empty_like(data) if tmp is None else tmp
     s = torch.cuda.current_stream().cuda_stream if cuda_stream is None else cuda_stream
     _check(f(vp(data.data_ptr()), X, Y, levels, vp(t.data_ptr()), vp(s)), "bpc_dwt53")
+
+
+class Server:
+    """The request server (bpc_server_*): encode and decode requests of mixed
+    size admitted in arrival order against a device-memory budget reserved
+    once, overlapped on up to `max_in_flight` streams by a native worker
+    thread.  Inputs are device tensors the caller keeps alive until their
+    request completes; outputs live in the server's budget until released."""
+
+    def __init__(self, budget_bytes: int, max_in_flight: int = 8):
+        L = lib()
+        vp, ll = ctypes.c_void_p, ctypes.c_longlong
+        L.bpc_server_create.argtypes = [ll, ctypes.c_int, ctypes.POINTER(vp)]
+        L.bpc_server_register_lut.argtypes = [vp, vp, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                              ctypes.POINTER(ctypes.c_int)]
+        L.bpc_server_submit.argtypes = [vp, ctypes.c_int, vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+        L.bpc_server_submit.restype = ll
+        L.bpc_server_cancel.argtypes = [vp, ll]
+        L.bpc_server_poll.argtypes = [vp, ctypes.c_int, ctypes.c_int, vp, vp, vp, vp, ctypes.POINTER(ctypes.c_int)]
+        L.bpc_server_release.argtypes = [vp, vp]
+        L.bpc_server_state.argtypes = [vp] + [ctypes.POINTER(ll)] * 4
+        L.bpc_server_destroy.argtypes = [vp]
+        self.L = L
+        h = vp()
+        _check(L.bpc_server_create(budget_bytes, max_in_flight, ctypes.byref(h)), "bpc_server_create")
+        self.h = h
+        self._cap = 0
+        self._grow(256)
+
+    def _grow(self, n: int) -> None:
+        if n > self._cap:
+            self._cap = n
+            self._t = np.zeros(n, np.int64)
+            self._o = np.zeros(n, np.uint64)
+            self._l = np.zeros(n, np.float64)
+            self._s = np.zeros(n, np.int32)
+
+    def register_lut(self, lut: DeviceLut) -> int:
+        i = ctypes.c_int()
+        _check(self.L.bpc_server_register_lut(self.h, ctypes.c_void_p(lut.ptr), lut.n, lut.passes, lut.levels,
+                                              ctypes.byref(i)), "bpc_server_register_lut")
+        return i.value
+
+    def submit(self, direction: int, data, lut_id: int, cb: int = 64, shape=None) -> int:
+        """Queue a request on device data (a torch tensor or a raw pointer
+        with `shape` = (Y, X)); returns the ticket or a negative error."""
+        Y, X = shape if shape is not None else data.shape
+        ptr = data if isinstance(data, int) else data.data_ptr()
+        return self.L.bpc_server_submit(self.h, direction, ctypes.c_void_p(ptr), X, Y, lut_id, cb)
+
+    def cancel(self, ticket: int) -> int:
+        return self.L.bpc_server_cancel(self.h, ticket)
+
+    def poll(self, max_n: int = 256, wait_us: int = 0):
+        """Finished requests as a list of (ticket, output pointer, latency us,
+        status)."""
+        self._grow(max_n)
+        n = ctypes.c_int()
+        _check(self.L.bpc_server_poll(self.h, max_n, wait_us, self._t.ctypes.data, self._o.ctypes.data,
+                                      self._l.ctypes.data, self._s.ctypes.data, ctypes.byref(n)), "bpc_server_poll")
+        k = n.value
+        return list(zip(self._t[:k].tolist(), self._o[:k].tolist(), self._l[:k].tolist(), self._s[:k].tolist()))
+
+    def release(self, output_ptr: int) -> None:
+        _check(self.L.bpc_server_release(self.h, ctypes.c_void_p(output_ptr)), "bpc_server_release")
+
+    def state(self) -> dict:
+        v = [ctypes.c_longlong() for _ in range(4)]
+        _check(self.L.bpc_server_state(self.h, *[ctypes.byref(x) for x in v]), "bpc_server_state")
+        return dict(zip(("queued", "in_flight", "bytes_used", "completed"), (x.value for x in v)))
+
+    def close(self) -> None:
+        if self.h:
+            self.L.bpc_server_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def as_tensor(ptr: int, n: int, device_index: int | None = None):
+    """A torch int32 view of `n` ints of device memory at `ptr` (no copy);
+    valid while the memory is (e.g. until the server output is released)."""
+    import torch
+
+    class _View:
+        __cuda_array_interface__ = {"shape": (n,), "typestr": "<i4", "data": (ptr, False), "version": 3}
+
+    dev = torch.cuda.current_device() if device_index is None else device_index
+    return torch.as_tensor(_View(), device=f"cuda:{dev}")

@@ -130,8 +130,10 @@ def synthetic_coefficients(side: int, levels: int, seed: int, amp: float = 20.0,
 
 def laplacian_coefficients(side: int, levels: int, seed: int, max_plane: int = 15) -> np.ndarray:
     """i.i.d. Laplacian coefficients, scale 2**(level+3) per subband (level 0 =
-    finest; LL uses level `levels`), magnitudes clipped below 2**(max_plane+1)
-    so that every plane up to `max_plane` is populated in the coarse bands."""
+    finest; LL uses level `levels`), magnitudes clipped below 2**(max_plane+1).
+    The scale alone rarely reaches the top planes; laplacian_coefficients_gpu
+    plants one top-plane coefficient per codeblock to make every codeblock
+    code all of them."""
     rng = np.random.default_rng(seed)
     out = np.zeros((side, side), np.int64)
     for lv in range(levels):
@@ -185,3 +187,36 @@ def synthetic_coefficients_gpu(side: int, levels: int, seed: int, amp: float = 2
     img = make_image_gpu(side, seed, amp, nrect) - 128
     bpc_paco.dwt53(img, levels, tmp=tmp)
     return img
+
+
+def laplacian_coefficients_gpu(side: int, levels: int, seed: int, max_plane: int = 15, cb: int = 64,
+                               device="cuda"):
+    """The Laplacian field of laplacian_coefficients generated with torch on the
+    GPU (its own RNG stream), plus, in every cb x cb codeblock, one coefficient
+    at a random position with magnitude in [2**max_plane, 2**(max_plane+1))
+    and a random sign: every codeblock then has MSB plane `max_plane` and codes
+    all max_plane + 1 magnitude bitplanes.  Returns an int32 tensor."""
+    import torch
+    g = torch.Generator(device=device).manual_seed(seed)
+    out = torch.empty((side, side), dtype=torch.float32, device=device)
+
+    def lap(h, scale):
+        u = torch.rand((h, h), generator=g, device=device) - 0.5
+        return -scale * torch.sign(u) * torch.log1p(-2.0 * u.abs())
+
+    for lv in range(levels):
+        h = side >> (lv + 1)
+        for (y0, x0) in ((0, h), (h, 0), (h, h)):
+            out[y0:y0 + h, x0:x0 + h] = lap(h, 2.0 ** (lv + 3))
+    h = side >> levels
+    out[:h, :h] = lap(h, 2.0 ** (levels + 3))
+    lim = (1 << (max_plane + 1)) - 1
+    out = torch.clamp(torch.round(out), -lim, lim).to(torch.int32)
+    n = side // cb
+    pos = torch.randint(0, cb * cb, (n, n), generator=g, device=device)
+    mag = torch.randint(1 << max_plane, 1 << (max_plane + 1), (n, n), generator=g, device=device, dtype=torch.int32)
+    sgn = torch.randint(0, 2, (n, n), generator=g, device=device, dtype=torch.int32) * 2 - 1
+    rows = (torch.arange(n, device=device)[:, None] * cb + pos // cb).reshape(-1)
+    cols = (torch.arange(n, device=device)[None, :] * cb + pos % cb).reshape(-1)
+    out[rows, cols] = (mag * sgn).reshape(-1)
+    return out

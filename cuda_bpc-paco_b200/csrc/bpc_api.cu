@@ -173,7 +173,8 @@ const char *bpc_status_string(int st) {
         case BPC_ERR_FILE: return "cannot open LUT file";
         case BPC_ERR_PARSE: return "malformed LUT file";
         case BPC_ERR_NOMEM: return "out of memory";
-        case BPC_ERR_TOO_LARGE: return "image larger than the no-allocation entry point's fixed scratch";
+        case BPC_ERR_TOO_LARGE: return "input larger than the fixed scratch or memory budget it must fit";
+        case BPC_ERR_CANCELLED: return "request cancelled";
         default: break;
     }
     if (st > 0) {

@@ -36,7 +36,9 @@ enum { BPC_CODE = 0, BPC_DECODE = 1 };
 #define BPC_ERR_FILE (-3)
 #define BPC_ERR_PARSE (-4)
 #define BPC_ERR_NOMEM (-5)
-#define BPC_ERR_TOO_LARGE (-6) /* image larger than bpc_encode_compact_noalloc's fixed scratch */
+#define BPC_ERR_TOO_LARGE (-6) /* image larger than bpc_encode_compact_noalloc's fixed scratch, or a
+                                  server request larger than the server's whole memory budget */
+#define BPC_ERR_CANCELLED (-7) /* server request withdrawn by bpc_server_cancel before it ran */
 #define BPC_ST_SLOT_OVERFLOW 1
 #define BPC_ST_BAD_STREAM 2
 #define BPC_ST_INPUT_RANGE 4
@@ -148,6 +150,45 @@ int bpc_batch_destroy(void *batch);
  * overlap on the GPU race, so serialise them. */
 int bpc_encode_compact_noalloc(const int *d_coeffs, int X, int Y, const int *d_lut, int lut_n, int passes, int levels,
                                int cb_size, int *d_compact, long long *d_offsets, int *d_status, void *stream);
+
+/* ---------------------------------------------------------------------------
+ * Request server (no counterpart in the reference, whose CUDA_BPC codes one
+ * image per synchronous call).  Encode and decode requests of mixed size,
+ * pass count, DWT depth and codeblock size are admitted in arrival order
+ * against a device-memory budget and run concurrently, one launch per request
+ * on up to max_in_flight streams, from a worker thread.
+ *
+ * Memory: bpc_server_create reserves budget_bytes of device memory once; each
+ * request's output (encode: the X*Y-int slot stream; decode: X*Y coefficients)
+ * is carved from it when the request is admitted and given back by
+ * bpc_server_release.  Nothing is allocated while requests are served.  Inputs
+ * (coefficients or slot streams) and LUTs are the caller's device buffers and
+ * must stay valid until the request completes.  Unlike the rest of this
+ * header, the bpc_server_* calls may be made from several host threads.
+ * ------------------------------------------------------------------------- */
+int bpc_server_create(long long budget_bytes, int max_in_flight, void **server);
+/* Register a device LUT (from bpc_load_luts) for a pass count and DWT depth;
+ * *lut_id names it in bpc_server_submit.  The server does not own it. */
+int bpc_server_register_lut(void *server, const int *d_lut, int lut_n, int passes, int levels, int *lut_id);
+/* Queue a request; returns its ticket (>= 0) or a negative BPC_ERR_*
+ * (BPC_ERR_TOO_LARGE when its output exceeds the whole budget). */
+long long bpc_server_submit(void *server, int direction, const int *d_in, int X, int Y, int lut_id, int cb_size);
+/* Withdraw a request that has not been admitted yet; it is then reported by
+ * bpc_server_poll with status BPC_ERR_CANCELLED and no output. */
+int bpc_server_cancel(void *server, long long ticket);
+/* Take up to max finished requests (waiting up to wait_us for the first):
+ * ticket, output (device; NULL if the request failed before running),
+ * latency from submission to completion in microseconds, and status (0, the
+ * OR of BPC_ST_* bits, or a negative BPC_ERR_*).  *n = number returned. */
+int bpc_server_poll(void *server, int max, int wait_us, long long *tickets, int **outputs, double *latency_us,
+                    int *status, int *n);
+/* Give a finished request's output back to the budget. */
+int bpc_server_release(void *server, const int *output);
+int bpc_server_state(void *server, long long *queued, long long *in_flight, long long *bytes_used,
+                     long long *completed);
+/* Drops queued requests, waits for those on the GPU, frees the budget (every
+ * output not yet released becomes invalid). */
+int bpc_server_destroy(void *server);
 
 /* Reversible CDF 5/3 lifting DWT (JPEG 2000 integer filter) on the GPU, in
  * place on an X x Y int32 raster, `levels` levels, Mallat layout (LL top-left,

@@ -15,7 +15,7 @@ def header_functions():
     text = open(os.path.join(ROOT, "include", "bpc_paco.h")).read()
     text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
     text = "\n".join(l for l in text.splitlines() if not l.lstrip().startswith("#"))
-    decl = r"^\s*(?:const\s+)?(?:void|int|char)\s*\**\s*([A-Za-z_]\w*)\s*\([^;{]*\)\s*;"
+    decl = r"^\s*(?:const\s+)?(?:void|int|char|long\s+long)\s*\**\s*([A-Za-z_]\w*)\s*\([^;{]*\)\s*;"
     return sorted(set(re.findall(decl, text, flags=re.M)))
 
 
