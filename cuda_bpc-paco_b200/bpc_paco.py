@@ -307,6 +307,53 @@ def dwt53(data, levels: int, inverse: bool = False, tmp=None, cuda_stream: int |
     _check(f(vp(data.data_ptr()), X, Y, levels, vp(t.data_ptr()), vp(s)), "bpc_dwt53")
 
 
+def save_cstreams(folder: str, stream: np.ndarray, X: int, Y: int, levels: int = 5, cb: int = 64) -> None:
+    """Write a host slot stream as per-codeblock .bin files (bpc_save_cstreams)."""
+    s = np.ascontiguousarray(stream, dtype=np.int32)
+    assert s.size == X * Y
+    L = lib()
+    L.bpc_save_cstreams.argtypes = [ctypes.c_char_p, ctypes.c_void_p] + [ctypes.c_int] * 4
+    _check(L.bpc_save_cstreams(_folder(folder), s.ctypes.data, X, Y, levels, cb), "bpc_save_cstreams")
+
+
+def load_cstreams(folder: str, X: int, Y: int, levels: int = 5, cb: int = 64, fill: int = -1) -> np.ndarray:
+    """Read per-codeblock .bin files into a slot stream (bpc_load_cstreams);
+    slots no file covers keep `fill`."""
+    s = np.full(X * Y, fill, np.int32)
+    L = lib()
+    L.bpc_load_cstreams.argtypes = [ctypes.c_char_p, ctypes.c_void_p] + [ctypes.c_int] * 4
+    _check(L.bpc_load_cstreams(_folder(folder), s.ctypes.data, X, Y, levels, cb), "bpc_load_cstreams")
+    return s
+
+
+def lut_stats(coeffs, passes: int, levels: int = 5, cb: int = 64, stats=None):
+    """LUT training counts of device coefficients (bpc_lut_stats), added to
+    `stats` (a torch uint64 tensor of 2 * bpc_lut_entries(passes, levels, 15),
+    created zeroed when None); returns it."""
+    import torch
+    L = lib()
+    vp = ctypes.c_void_p
+    L.bpc_lut_stats.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp, vp]
+    n = L.bpc_lut_entries(passes, levels, 15)
+    if stats is None:
+        stats = torch.zeros(2 * n, dtype=torch.uint64, device=coeffs.device)
+    assert stats.numel() == 2 * n
+    Y, X = coeffs.shape
+    s = torch.cuda.current_stream().cuda_stream
+    _check(L.bpc_lut_stats(_ptr(coeffs), X, Y, passes, levels, cb, _ptr(stats), vp(s)), "bpc_lut_stats")
+    return stats
+
+
+def lut_write(folder: str, stats: np.ndarray, passes: int, levels: int = 5) -> None:
+    """Write LUT text files from host training counts (bpc_lut_write)."""
+    st = np.ascontiguousarray(stats, dtype=np.uint64)
+    L = lib()
+    L.bpc_lut_write.argtypes = [ctypes.c_char_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
+    assert st.size == 2 * L.bpc_lut_entries(passes, levels, 15)
+    os.makedirs(folder, exist_ok=True)
+    _check(L.bpc_lut_write(_folder(folder), st.ctypes.data, passes, levels), "bpc_lut_write")
+
+
 class Server:
     """The request server (bpc_server_*): encode and decode requests of mixed
     size admitted in arrival order against a device-memory budget reserved

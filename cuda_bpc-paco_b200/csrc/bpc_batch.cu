@@ -50,6 +50,7 @@ struct GpuWarpB {
     __device__ __forceinline__ int lane() const { return (int)(threadIdx.x & 31u); }
     __device__ __forceinline__ uint32_t ballot(bool p) { return __ballot_sync(0xffffffffu, p); }
     __device__ __forceinline__ bool any(bool p) { return __any_sync(0xffffffffu, p) != 0; }
+    __device__ __forceinline__ uint32_t reduce_or(uint32_t v) { return __reduce_or_sync(0xffffffffu, v); }
     __device__ __forceinline__ uint32_t shfl_xor(uint32_t v, int o) { return __shfl_xor_sync(0xffffffffu, v, o); }
     __device__ __forceinline__ uint32_t shfl_up(uint32_t v, int d) { return __shfl_up_sync(0xffffffffu, v, d); }
     __device__ __forceinline__ uint32_t shfl_down(uint32_t v, int d) { return __shfl_down_sync(0xffffffffu, v, d); }

@@ -114,6 +114,20 @@ BPC_FI int popc32(uint32_t x) {
     return __builtin_popcount(x);
 #endif
 }
+BPC_FI int popc64(uint64_t x) {
+#if defined(__CUDA_ARCH__)
+    return __popcll(x);
+#else
+    return __builtin_popcountll(x);
+#endif
+}
+BPC_FI void add_u64(unsigned long long *p, unsigned long long v) {
+#if defined(__CUDA_ARCH__)
+    atomicAdd(p, v);
+#else
+    *p += v;
+#endif
+}
 BPC_FI int ctz64(uint64_t x) {
 #if defined(__CUDA_ARCH__)
     return __ffsll((long long)x) - 1;
@@ -218,12 +232,7 @@ struct Lane {
 
 template <class W>
 BPC_FI uint64_t warp_or64(W &w, uint64_t v) {
-#pragma unroll
-    for (int o = 16; o; o >>= 1) {
-        uint32_t lo = w.shfl_xor((uint32_t)v, o), hi = w.shfl_xor((uint32_t)(v >> 32), o);
-        v |= ((uint64_t)hi << 32) | lo;
-    }
-    return v;
+    return ((uint64_t)w.reduce_or((uint32_t)(v >> 32)) << 32) | w.reduce_or((uint32_t)v);
 }
 
 template <class W>
@@ -762,10 +771,19 @@ struct Coder {
         s.C[1] |= cand1 & ~K[1];
     }
 
+    // One pass = masks (what is coded, with which context and symbol), code
+    // (the lane's arithmetic coder over those symbols, events ranked) and
+    // commit (the state the next pass sees).  LUT training replaces the code
+    // step with stats_pass.
     template <int PK>
     BPC_FI void enc_pass(int b, bool act) {
-        const int off = PK == PK_CP ? p.cp_off : 0;
-        const int sig_b = off + p.a_sig + (g + b) * 9, sign_b = off + p.a_sign + (g + b) * 4;
+        enc_pass_masks<PK>(b, act);
+        enc_pass_code<PK>(b, act);
+        enc_pass_commit<PK>(act);
+    }
+
+    template <int PK>
+    BPC_FI void enc_pass_masks(int b, bool act) {
         // The data bit coded at plane b is magnitude bit b for b <= 27; above
         // that the reference reads its flag bits (b+1 = 29 refinement, 30 CP,
         // 31 significance, >= 32 nothing), which for the coefficients each pass
@@ -800,6 +818,12 @@ struct Coder {
             enc_contexts();
             enc_sign_slices();
         }
+    }
+
+    template <int PK>
+    BPC_FI void enc_pass_code(int b, bool act) {
+        const int off = PK == PK_CP ? p.cp_off : 0;
+        const int sig_b = off + p.a_sig + (g + b) * 9, sign_b = off + p.a_sign + (g + b) * 4;
         const uint32_t Pref = PK == PK_MRP && act ? (uint32_t)tab[g + b] : 0u;
         // one lane's coded symbols in scan order: 16 rows at a time, the two
         // columns interleaved so that position t = 2*row + column
@@ -836,6 +860,10 @@ struct Coder {
             } while (kq);
         }
         enc_rank();
+    }
+
+    template <int PK>
+    BPC_FI void enc_pass_commit(bool act) {
         if (PK == PK_MRP) {
             if (act) {
                 s.R[0] = s.S[0];
@@ -855,8 +883,63 @@ struct Coder {
         }
     }
 
+    // LUT training (no counterpart in the reference, whose tables come
+    // pre-trained): for every LUT entry the pass uses, the number of symbols
+    // coded with it and how many of them were 1, counted bit-parallel from
+    // the pass masks.  Planes 0..14 only -- the planes of the LUT files, where
+    // each entry belongs to exactly one (level, subband, plane, context).
+    BPC_FI void tally(unsigned long long *st, int idx, uint32_t n, uint32_t ones) {
+        if (n) add_u64(st + 2 * idx, n);
+        if (ones) add_u64(st + 2 * idx + 1, ones);
+    }
+    template <int PK>
+    BPC_FI void stats_pass(int b, bool act, unsigned long long *st) {
+        if (!act || b >= 15) return;
+        const int off = PK == PK_CP ? p.cp_off : 0;
+        if (PK == PK_MRP) {
+            tally(st, g + b, (uint32_t)(popc64(K[0]) + popc64(K[1])), (uint32_t)(popc64(Y[0]) + popc64(Y[1])));
+        } else {
+            stats_ctx(st, off, b);
+        }
+    }
+    BPC_FI void stats_ctx(unsigned long long *st, int off, int b) {
+#pragma unroll 1
+        for (int k = 0; k < 9; k++) {
+            uint32_t n = 0, ones = 0;
+#pragma unroll
+            for (int c = 0; c < 2; c++) {
+                uint64_t m = K[c];
+#pragma unroll
+                for (int q = 0; q < 4; q++) m &= ((k >> q) & 1) ? cs[c][q] : ~cs[c][q];
+                n += (uint32_t)popc64(m);
+                ones += (uint32_t)popc64(m & Y[c]);
+            }
+            tally(st, off + p.a_sig + (g + b) * 9 + k, n, ones);
+        }
+#pragma unroll 1
+        for (int k = 0; k < 4; k++) {
+            uint32_t n = 0, ones = 0;
+#pragma unroll
+            for (int c = 0; c < 2; c++) {
+                const uint64_t m = NS[c] & ((k & 1) ? si[c][0] : ~si[c][0]) & ((k & 2) ? si[c][1] : ~si[c][1]);
+                n += (uint32_t)popc64(m);
+                ones += (uint32_t)popc64(m & sg[c]);
+            }
+            tally(st, off + p.a_sign + (g + b) * 4 + k, n, ones);
+        }
+    }
+    template <int PK>
+    BPC_FI void train_pass(int b, bool act, unsigned long long *st) {
+        enc_pass_masks<PK>(b, act);
+        stats_pass<PK>(b, act, st);
+        enc_pass_commit<PK>(act);
+    }
+
     // ------------------------------------------------------ codeblock driver
-    BPC_FI void run(int cb_first) {
+    // STATS (encoder only): gather LUT training counts into `stats` instead of
+    // writing the slot stream.
+    template <bool STATS = false>
+    BPC_FI void run(int cb_first, unsigned long long *stats = nullptr) {
         const int grp = lane / G::NL;
         const int cb = cb_first + grp;
         const bool ok = cb < p.cb_end;
@@ -911,7 +994,7 @@ struct Coder {
             for (int o = G::NL / 2; o; o >>= 1) mx |= w.shfl_xor(mx, o);
             if (ok) {
                 msb = mx ? 31 - clz32(mx) : 32;
-                if (gl == 0) slot_out[0] = msb;  // :1155
+                if (gl == 0 && !STATS) slot_out[0] = msb;  // :1155
                 // bitplanes 0..min(MSB, 27): transpose 32 rows x 32 bits at a time
                 top = msb <= 27 ? msb : -1;
                 if (top >= 0) {
@@ -973,7 +1056,13 @@ struct Coder {
             const bool full = PASSES == 2 ? b <= msb : b < msb;
             const bool first_cp = PASSES == 3 && b == msb;
             plane_begin(b);
-            if (ENC) {
+            if (ENC && STATS) {
+                if (w.any(full)) {
+                    train_pass<PK_SPP>(b, full, stats);
+                    train_pass<PK_MRP>(b, full, stats);
+                }
+                if (PASSES == 3 && w.any(full || first_cp)) train_pass<PK_CP>(b, full || first_cp, stats);
+            } else if (ENC) {
                 if (w.any(full)) {
                     enc_pass<PK_SPP>(b, full);
                     enc_pass<PK_MRP>(b, full);
@@ -989,7 +1078,7 @@ struct Coder {
             if (b <= msb) plane_end(b);
         }
         if (ENC) {
-            if (ok) {
+            if (ok && !STATS) {
                 if (s.has_resv && s.size != 0) {  // flush :1020 (a finished codeword is already stored)
                     if (s.open_slot < G::CAP)
                         slot_out[s.open_slot] = (int32_t)s.lower;

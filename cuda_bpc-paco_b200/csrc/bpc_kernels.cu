@@ -18,6 +18,7 @@ struct GpuWarp {
     __device__ __forceinline__ int lane() const { return (int)(threadIdx.x & 31u); }
     __device__ __forceinline__ uint32_t ballot(bool p) { return __ballot_sync(0xffffffffu, p); }
     __device__ __forceinline__ bool any(bool p) { return __any_sync(0xffffffffu, p) != 0; }
+    __device__ __forceinline__ uint32_t reduce_or(uint32_t v) { return __reduce_or_sync(0xffffffffu, v); }
     __device__ __forceinline__ uint32_t shfl_xor(uint32_t v, int o) { return __shfl_xor_sync(0xffffffffu, v, o); }
     __device__ __forceinline__ uint32_t shfl_up(uint32_t v, int d) { return __shfl_up_sync(0xffffffffu, v, d); }
     __device__ __forceinline__ uint32_t shfl_down(uint32_t v, int d) { return __shfl_down_sync(0xffffffffu, v, d); }
@@ -73,6 +74,41 @@ __global__ void __launch_bounds__(kWarps * 32, ENC ? kMinCtasEnc : kMinCtasDec) 
         Coder<PASSES, CBS, ENC, GpuWarp> cd(w, p, ring, tab, planes, ev_key, ev_val);
         cd.run(base);
     }
+}
+
+// LUT training counts: the encoder's pass masks without its arithmetic coder
+template <int PASSES, int CBS>
+__global__ void __launch_bounds__(kWarps * 32, kMinCtasEnc) k_bpc_stats(Params p, unsigned long long *stats) {
+    using G = Geo<CBS>;
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int warp = (int)(threadIdx.x >> 5);
+    uint32_t *ring = reinterpret_cast<uint32_t *>(smem) + warp * 512;
+    GpuWarp w;
+    uint32_t planes[28][4];
+    uint8_t ev_key[1];
+    uint32_t ev_val[1];
+    const int stride = (int)gridDim.x * kWarps * G::NG;
+    for (int base = p.cb_begin + ((int)blockIdx.x * kWarps + warp) * G::NG; base < p.cb_end; base += stride) {
+        Coder<PASSES, CBS, true, GpuWarp> cd(w, p, ring, nullptr, planes, ev_key, ev_val);
+        cd.template run<true>(base, stats);
+    }
+}
+
+template <int PASSES, int CBS>
+static cudaError_t launch_stats_t(const Params &p, unsigned long long *stats, cudaStream_t st) {
+    using G = Geo<CBS>;
+    const size_t sm = (size_t)kWarps * 4u * 512u;
+    const int warps_needed = (p.cb_end - p.cb_begin + G::NG - 1) / G::NG;
+    const int grid = (warps_needed + kWarps - 1) / kWarps;
+    if (grid < 1) return cudaSuccess;
+    k_bpc_stats<PASSES, CBS><<<grid, kWarps * 32, sm, st>>>(p, stats);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_stats(int passes, int cbs, const Params &p, unsigned long long *stats, cudaStream_t st) {
+    if (p.cb_end <= p.cb_begin) return cudaSuccess;
+    if (passes == 2) return cbs == 64 ? launch_stats_t<2, 64>(p, stats, st) : launch_stats_t<2, 32>(p, stats, st);
+    return cbs == 64 ? launch_stats_t<3, 64>(p, stats, st) : launch_stats_t<3, 32>(p, stats, st);
 }
 
 template <int PASSES, int CBS, bool ENC>

@@ -24,4 +24,8 @@ constexpr int kMinCtasEnc = ENC_MIN_CTAS;
 // walk the codeblocks grid-stride.
 cudaError_t launch_code(bool enc, int passes, int cbs, const Params &p, int grid, cudaStream_t st);
 
+// LUT training: add, per LUT entry, [2k] symbols coded and [2k+1] symbols
+// equal to 1 over p.ncb codeblocks of p.in (planes 0..14) to stats.
+cudaError_t launch_stats(int passes, int cbs, const Params &p, unsigned long long *stats, cudaStream_t st);
+
 }  // namespace bpc

@@ -14,12 +14,16 @@
 // is one launch of the plain coder on its own stream, followed by a 4-byte
 // copy of its status word and an event; launches on different streams run
 // concurrently, so the CTAs of a newly admitted request fill the SMs that an
-// earlier request's tail leaves idle.  Each slot has one stream per hardware
-// priority level and a request runs on the level of its size (2^22
-// coefficients or fewer on the highest, one level lower per doubling): the
-// block scheduler then dispatches a small request's CTAs ahead of the
-// not-yet-started CTAs of a large one, so small requests are not stuck behind
-// large ones (running CTAs are never preempted).  A worker thread admits
+// earlier request's tail leaves idle.  Each slot has one stream per priority
+// class (up to three hardware priority levels) and a request runs in the class
+// of its size (up to 2^22 coefficients; up to 2^24; larger): the block
+// scheduler then dispatches a small request's CTAs ahead of the not-yet-started
+// CTAs of a large one, so small requests are not stuck behind large ones
+// (running CTAs are never preempted).  The device feeds streams through a
+// limited number of hardware queues (CUDA_DEVICE_MAX_CONNECTIONS, 8 unless the
+// process sets it before CUDA initialises); streams that share a queue run in
+// order, so a process serving small requests beside large ones should set it
+// to 32 (8 slots x 3 classes = 24 streams).  A worker thread admits
 // requests and polls the events; the latency of a request is measured on the
 // host clock from its submission to the moment the worker sees its event
 // complete.
@@ -139,12 +143,15 @@ struct Server {
 
 constexpr size_t kAlign = 256;
 
-// priority level of a request: 0 (highest) up to 2^22 coefficients, one lower per doubling
+constexpr int kMaxClasses = 3;
+
+// priority class of a request: 0 (highest) up to 2^22 coefficients, 1 up to
+// 2^24, 2 above
 int priority_level(int X, int Y, int nprio) {
     const unsigned long long n = (unsigned long long)X * (unsigned long long)Y;
     int lg = 0;
     while ((2ULL << lg) <= n) ++lg;  // floor(log2(n))
-    const int p = lg - 22;
+    const int p = (lg - 21) / 2;
     return p < 0 ? 0 : (p >= nprio ? nprio - 1 : p);
 }
 
@@ -248,7 +255,8 @@ extern "C" int bpc_server_create(long long budget_bytes, int max_in_flight, void
     bool ok = cudaDeviceGetStreamPriorityRange(&least, &greatest) == cudaSuccess &&
               cudaMalloc(&s->d_status, sizeof(int) * max_in_flight) == cudaSuccess &&
               cudaHostAlloc(&s->h_status, sizeof(int) * max_in_flight, cudaHostAllocDefault) == cudaSuccess;
-    const int nprio = ok ? (least - greatest + 1 < 1 ? 1 : least - greatest + 1) : 1;
+    int nprio = ok ? least - greatest + 1 : 1;
+    nprio = nprio < 1 ? 1 : (nprio > kMaxClasses ? kMaxClasses : nprio);
     for (int k = 0; ok && k < max_in_flight; ++k) {
         Slot &sl = s->slots[k];
         sl.d_status = s->d_status + k;

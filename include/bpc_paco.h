@@ -165,6 +165,10 @@ int bpc_encode_compact_noalloc(const int *d_coeffs, int X, int Y, const int *d_l
  * (coefficients or slot streams) and LUTs are the caller's device buffers and
  * must stay valid until the request completes.  Unlike the rest of this
  * header, the bpc_server_* calls may be made from several host threads.
+ * Requests run on streams of three priority classes by size (small first);
+ * set CUDA_DEVICE_MAX_CONNECTIONS=32 in the environment before CUDA
+ * initialises so that these streams do not share hardware queues (with the
+ * default 8, a small request can wait behind a large one in the same queue).
  * ------------------------------------------------------------------------- */
 int bpc_server_create(long long budget_bytes, int max_in_flight, void **server);
 /* Register a device LUT (from bpc_load_luts) for a pass count and DWT depth;
@@ -189,6 +193,44 @@ int bpc_server_state(void *server, long long *queued, long long *in_flight, long
 /* Drops queued requests, waits for those on the GPU, frees the budget (every
  * output not yet released becomes invalid). */
 int bpc_server_destroy(void *server);
+
+/* ---------------------------------------------------------------------------
+ * Per-codeblock stream files: the reference's load_CStream
+ * (source/main_example.cu:51-68) over the file numbering of its load_Data
+ * (:71-179).  File k is "<folder><k>.bin" (folder is a prefix, normally ending
+ * in '/'): the cb_size*cb_size words of one codeblock's slot as 16-bit
+ * big-endian values.  Files are numbered LL band first, then for level =
+ * levels..1 the HL, LH and HH bands, each in raster order of codeblocks; file
+ * k belongs to the slot of the codeblock at that position.  On reading, a byte
+ * past the end of a file makes its word -1 (as fgetc's EOF does in the
+ * reference); a missing file returns BPC_ERR_FILE.  The -1 fill of a slot is
+ * written as 0xFFFF and reads back as 65535 (a decoder never reads it).
+ * ------------------------------------------------------------------------- */
+int bpc_load_cstreams(const char *folder, int *stream, int X, int Y, int levels, int cb_size);
+int bpc_save_cstreams(const char *folder, const int *stream, int X, int Y, int levels, int cb_size);
+/* Number of files the two calls above read or write for this geometry. */
+int bpc_cstream_files(int X, int Y, int levels, int cb_size);
+
+/* ---------------------------------------------------------------------------
+ * LUT training (no counterpart in the reference, which ships trained tables
+ * but no trainer).  A LUT entry is the probability, out of 128, that the
+ * symbol coded with it is 0.  bpc_lut_stats adds to d_stats (device, 2 *
+ * bpc_lut_entries(passes, levels, 15) unsigned 64-bit counters, zeroed by the
+ * caller before the first image) the number of symbols the encoder codes with
+ * each entry on the X x Y coefficients d_coeffs ([2k]) and how many of them
+ * are 1 ([2k+1]), over planes 0..14; call it once per training image.
+ * bpc_lut_write turns host counts into ref.txt, sig.txt, sign.txt (+ cp_sig.txt,
+ * cp_sign.txt for 3 passes) in `folder` (a prefix, normally ending in '/'):
+ * P = round(128 * zeros / symbols) clamped to 1..127, 64 where no symbol was
+ * coded, each (level, subband) group listing planes up to one past its last
+ * used plane, which is written as all 64 (the shipped tables' convention;
+ * load_LUTs overwrites the last listed plane of a group with 64 after its
+ * first entry), and the LL group listing all 15 planes so that load_LUTs
+ * builds the 15-plane layout.  The files load with load_LUTs / bpc_load_luts.
+ * ------------------------------------------------------------------------- */
+int bpc_lut_stats(const int *d_coeffs, int X, int Y, int passes, int levels, int cb_size,
+                  unsigned long long *d_stats, void *stream);
+int bpc_lut_write(const char *folder, const unsigned long long *h_stats, int passes, int levels);
 
 /* Reversible CDF 5/3 lifting DWT (JPEG 2000 integer filter) on the GPU, in
  * place on an X x Y int32 raster, `levels` levels, Mallat layout (LL top-left,

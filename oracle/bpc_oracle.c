@@ -277,9 +277,21 @@ typedef struct {
     long counter;
     int status;
     int ref_quirk; /* decoder follows the reference decoder exactly */
+    uint64_t *stats; /* LUT training counts, or NULL */
+    long stats_n;
 } cbstate;
 
 static inline int lut_get(const cbstate *c, long idx) { return (idx >= 0 && idx < c->lut_n) ? c->lut[idx] : 0; }
+
+/* LUT training counts (no counterpart in the reference): per LUT entry, the
+ * symbols coded with it and how many were 1, for planes 0..14 (the planes of
+ * the LUT files, where each entry belongs to one level/subband/plane/context). */
+static inline void tally(cbstate *c, long idx, uint32_t sym, int b) {
+    if (c->stats && b < NBP && idx >= 0 && idx < c->stats_n) {
+        c->stats[2 * idx]++;
+        c->stats[2 * idx + 1] += sym;
+    }
+}
 
 /* Neighbour word at (row, global column) of the codeblock, 0 outside: the
  * shuffles of Share_{Left,Right}_Borders (:342-388) plus the zeroing of row 0 /
@@ -374,6 +386,7 @@ static int spp_enc_sig(cbstate *c, int l, int r, int col, int b, int *sctx) {
     }
     lut_ptrs p = lut_at_plane(c->lvl[l], c->sb[l], b, c->levels);
     int ctx = sig_context(c, r, gc);
+    tally(c, p.sig + ctx, shr32(*w, b + 1) & 1, b);
     ac_encode(c, l, shr32(*w, b + 1) & 1, lut_get(c, p.sig + ctx));
     if ((shr32(*w, b + 1) & 1) == 1) {
         *w |= SIGMA;
@@ -391,6 +404,7 @@ static int cp_enc_sig(cbstate *c, int l, int r, int col, int b, int *sctx) {
     if (!((*w >> 30) & 1)) return 0;
     lut_ptrs p = lut_at_plane(c->lvl[l], c->sb[l], b, c->levels);
     int ctx = sig_context(c, r, gc);
+    tally(c, p.sig + p.cp_off + ctx, shr32(*w, b + 1) & 1, b);
     ac_encode(c, l, shr32(*w, b + 1) & 1, lut_get(c, p.sig + p.cp_off + ctx));
     *w &= ~CPF;
     if ((shr32(*w, b + 1) & 1) == 1) {
@@ -405,14 +419,17 @@ static void enc_sign(cbstate *c, int l, int r, int col, int b, int sctx, int cp)
     uint32_t w = c->T[l][2 * r + col];
     lut_ptrs p = lut_at_plane(c->lvl[l], c->sb[l], b, c->levels);
     long base = p.sign + (cp ? p.cp_off : 0);
+    tally(c, base + (sctx >> 1), ((w & 1) == (uint32_t)(sctx & 1)) ? 0u : 1u, b);
     ac_encode(c, l, ((w & 1) == (uint32_t)(sctx & 1)) ? 0u : 1u, lut_get(c, base + (sctx >> 1)));
 }
 
 /* MRP_Encoder :593-605 */
-static void mrp_enc(cbstate *c, int l, int r, int col, int b, int P) {
+static void mrp_enc(cbstate *c, int l, int r, int col, int b, long idx) {
     uint32_t *w = &c->T[l][2 * r + col];
-    if ((*w >> 29) & 1)
-        ac_encode(c, l, shr32(*w, b + 1) & 1, P);
+    if ((*w >> 29) & 1) {
+        tally(c, idx, shr32(*w, b + 1) & 1, b);
+        ac_encode(c, l, shr32(*w, b + 1) & 1, lut_get(c, idx));
+    }
     else if (*w >> 31)
         *w |= REFF;
 }
@@ -435,7 +452,7 @@ static void enc_mrp_pass(cbstate *c, int b) {
         for (int col = 0; col < 2; col++)
             for (int l = 0; l < c->nl; l++) {
                 lut_ptrs p = lut_at_plane(c->lvl[l], c->sb[l], b, c->levels);
-                mrp_enc(c, l, r, col, b, lut_get(c, p.ref));
+                mrp_enc(c, l, r, col, b, p.ref);
             }
 }
 
@@ -541,6 +558,8 @@ typedef struct {
     long ncb, next;
     pthread_mutex_t mu;
     int any_status;
+    uint64_t *stats; /* LUT training counts (summed over the workers), or NULL */
+    long stats_n;
 } job;
 
 static void setup_geometry(cbstate *c, const job *j, long k, int *x0, int *y0) {
@@ -667,6 +686,8 @@ static void *worker(void *p) {
     worker_arg *a = (worker_arg *)p;
     job *j = a->j;
     cbstate *c = (cbstate *)malloc(sizeof(cbstate));
+    c->stats = j->stats ? (uint64_t *)calloc((size_t)(2 * j->stats_n), sizeof(uint64_t)) : NULL;
+    c->stats_n = j->stats_n;
     int st_all = 0;
     for (;;) {
         pthread_mutex_lock(&j->mu);
@@ -682,15 +703,19 @@ static void *worker(void *p) {
             st_all |= st;
         }
     }
-    free(c);
     pthread_mutex_lock(&j->mu);
     j->any_status |= st_all;
+    if (c->stats)
+        for (long q = 0; q < 2 * j->stats_n; q++) j->stats[q] += c->stats[q];
     pthread_mutex_unlock(&j->mu);
+    free(c->stats);
+    free(c);
     return NULL;
 }
 
 static int run(int enc, const int32_t *in, int32_t *out, int X, int Y, const int *lut, int lut_n, int passes,
-               int levels, int cb, int nthreads, int32_t *status, int ref_quirk, long cb_begin, long cb_end) {
+               int levels, int cb, int nthreads, int32_t *status, int ref_quirk, long cb_begin, long cb_end,
+               uint64_t *stats, long stats_n) {
     if (!in || !out || !lut || X <= 0 || Y <= 0 || (passes != 2 && passes != 3) || levels < 1 ||
         (cb != 64 && cb != 32) || X % cb || Y % cb)
         return BPCO_ERR_ARG;
@@ -707,6 +732,8 @@ static int run(int enc, const int32_t *in, int32_t *out, int X, int Y, const int
     j.out = out;
     j.status = status;
     j.ref_quirk = ref_quirk;
+    j.stats = stats;
+    j.stats_n = stats_n;
     long ncb = (long)(X / cb) * (Y / cb);
     if (cb_end < 0 || cb_end > ncb) cb_end = ncb;
     if (cb_begin < 0) cb_begin = 0;
@@ -728,13 +755,35 @@ static int run(int enc, const int32_t *in, int32_t *out, int X, int Y, const int
  * Returns the OR of the per-codeblock status bits, or a negative error. */
 int bpco_encode(const int32_t *img, int32_t *stream, int X, int Y, const int *lut, int lut_n, int passes, int levels,
                 int cb, int nthreads, int32_t *status, long cb_begin, long cb_end) {
-    return run(1, img, stream, X, Y, lut, lut_n, passes, levels, cb, nthreads, status, 0, cb_begin, cb_end);
+    return run(1, img, stream, X, Y, lut, lut_n, passes, levels, cb, nthreads, status, 0, cb_begin, cb_end, NULL, 0);
 }
 
 int bpco_decode(const int32_t *stream, int32_t *img, int X, int Y, const int *lut, int lut_n, int passes, int levels,
                 int cb, int nthreads, int32_t *status, int ref_quirk, long cb_begin, long cb_end) {
     return run(0, stream, img, X, Y, lut, lut_n, passes, levels, cb, nthreads, status, ref_quirk, cb_begin,
-               cb_end);
+               cb_end, NULL, 0);
+}
+
+/* LUT training counts of an image: adds, for every entry of the LUT layout
+ * with 15 planes (stats_n entries), stats[2k] += symbols coded with entry k
+ * and stats[2k+1] += those equal to 1, over planes 0..14.  The encoder runs
+ * with an all-64 table (the counts do not depend on the probabilities). */
+int bpco_lut_stats(const int32_t *img, int X, int Y, int passes, int levels, int cb, int nthreads, uint64_t *stats,
+                   long stats_n) {
+    if (!stats || stats_n <= 0) return BPCO_ERR_ARG;
+    int *lut = (int *)malloc(sizeof(int) * (size_t)stats_n);
+    int32_t *scratch = (int32_t *)malloc(sizeof(int32_t) * (size_t)X * (size_t)Y);
+    if (!lut || !scratch) {
+        free(lut);
+        free(scratch);
+        return BPCO_ERR_ARG;
+    }
+    for (long q = 0; q < stats_n; q++) lut[q] = 64;
+    int rc = run(1, img, scratch, X, Y, lut, (int)stats_n, passes, levels, cb, nthreads, NULL, 0, 0, -1, stats,
+                 stats_n);
+    free(lut);
+    free(scratch);
+    return rc < 0 ? rc : 0;
 }
 
 /* MSB of a codeblock as the kernel computes it (Find_MSB :114-161); for the

@@ -52,6 +52,9 @@ def lib():
         L.bpco_find_subband.restype = None
         L.bpco_block_msb.argtypes = [i32p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int]
         L.bpco_block_msb.restype = ctypes.c_int
+        L.bpco_lut_stats.argtypes = [i32p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                     ctypes.c_int, ctypes.c_void_p, ctypes.c_long]
+        L.bpco_lut_stats.restype = ctypes.c_int
         _lib = L
     return _lib
 
@@ -114,3 +117,23 @@ def find_subband(x: int, y: int, X: int, Y: int, levels: int):
 def block_msb(img: np.ndarray, x0: int, y0: int, cb: int, passes: int) -> int:
     img = np.ascontiguousarray(img, dtype=np.int32)
     return lib().bpco_block_msb(_p(img), img.shape[1], x0, y0, cb, passes)
+
+
+def lut_entries(passes: int, levels: int, planes: int = 15) -> int:
+    """Entries of the load_LUTs layout: sections ref, sig, sign [, cp_sig,
+    cp_sign] of 3 * planes * N * levels + planes * N ints each."""
+    ns = [1, 9, 4] + ([9, 4] if passes == 3 else [])
+    return sum(3 * planes * n * levels + planes * n for n in ns)
+
+
+def lut_stats(img: np.ndarray, passes: int, levels: int = 5, cb: int = 64, threads: int = 0) -> np.ndarray:
+    """LUT training counts of one image: uint64 array of 2 * lut_entries,
+    [2k] symbols coded with entry k, [2k+1] of them equal to 1 (planes 0..14)."""
+    img = np.ascontiguousarray(img, dtype=np.int32)
+    Y, X = img.shape
+    n = lut_entries(passes, levels)
+    st = np.zeros(2 * n, np.uint64)
+    rc = lib().bpco_lut_stats(_p(img), X, Y, passes, levels, cb, threads or os.cpu_count() or 1, st.ctypes.data, n)
+    if rc < 0:
+        raise ValueError(f"oracle lut_stats: bad arguments ({rc})")
+    return st
