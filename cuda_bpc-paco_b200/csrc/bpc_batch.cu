@@ -97,7 +97,12 @@ __global__ void __launch_bounds__(kWarps * 32, ENC ? kMinCtasEnc : kMinCtasDec)
     using G = Geo<CBS>;
     extern __shared__ __align__(16) unsigned char smem[];
     const int warp = (int)(threadIdx.x >> 5);
-    uint32_t *ring = reinterpret_cast<uint32_t *>(smem) + warp * (ENC ? 512 : G::RING_WORDS);
+    uint8_t *sgtab = smem;
+    if (!ENC) {
+        build_sign_table(sgtab, (int)threadIdx.x, (int)blockDim.x);
+        __syncthreads();
+    }
+    uint32_t *ring = reinterpret_cast<uint32_t *>(smem + kSignTableBytes) + warp * (ENC ? 512 : G::RING_WORDS);
     GpuWarpB w;
     uint32_t planes[28][4];
     uint8_t ev_key[ENC ? 256 : 1];
@@ -129,7 +134,7 @@ __global__ void __launch_bounds__(kWarps * 32, ENC ? kMinCtasEnc : kMinCtasDec)
         p.cb_begin = 0;
         p.cb_end = im.ncb;
         for (int k = 0; k < item.n; k += G::NG) {
-            Coder<PASSES, CBS, ENC, GpuWarpB> cd(w, p, ring, im.tab, planes, ev_key, ev_val);
+            Coder<PASSES, CBS, ENC, GpuWarpB> cd(w, p, ring, im.tab, sgtab, planes, ev_key, ev_val);
             cd.run(item.cb0 + k);
         }
     }
@@ -260,7 +265,7 @@ template <int PASSES, int CBS, bool ENC>
 cudaError_t launch_batch(const Batch &b, int cls, const BatchImage *imgs, const long long *offsets, int *status,
                          cudaStream_t st) {
     using G = Geo<CBS>;
-    const size_t sm = (size_t)kWarps * 4u * (size_t)(ENC ? 512 : G::RING_WORDS);
+    const size_t sm = (size_t)kSignTableBytes + (size_t)kWarps * 4u * (size_t)(ENC ? 512 : G::RING_WORDS);
     cudaError_t e = cudaFuncSetAttribute(k_bpc_batch<PASSES, CBS, ENC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)sm);
     if (e != cudaSuccess) return e;

@@ -45,6 +45,23 @@ enum : int { PK_SPP = 0, PK_MRP = 1, PK_CP = 2 };
 constexpr uint32_t kSignTab = (0u << 0) | (2u << 3) | (3u << 6) | (4u << 9) | (6u << 12) | (0u << 15) |
                               (5u << 18) | (1u << 21) | (7u << 24);
 
+// The decoder's sign-context table: entry k for the neighbour bits
+// k = sl | nl<<1 | sr<<2 | nr<<3 | su<<4 | nu<<5 | sb<<6 | nb<<7 (s = significant,
+// n = negative; left, right, up, below) holds the LUT index (ctx >> 1) in bits
+// 0-1 and the predicted sign (ctx & 1) in bit 2.  Threads tid, tid + n, ...
+// fill it.
+constexpr int kSignTableBytes = 256;
+BPC_FI void build_sign_table(uint8_t *t, int tid, int n) {
+    for (int k = tid; k < kSignTableBytes; k += n) {
+        const int sl = k & 1, nl = (k >> 1) & 1, sr = (k >> 2) & 1, nr = (k >> 3) & 1;
+        const int su = (k >> 4) & 1, nu = (k >> 5) & 1, sb = (k >> 6) & 1, nb = (k >> 7) & 1;
+        const int h = sl * (1 - 2 * nl) + sr * (1 - 2 * nr), v = su * (1 - 2 * nu) + sb * (1 - 2 * nb);
+        const int hc = h == 0 ? 0 : (h > 0 ? 1 : 2), vc = v == 0 ? 0 : (v > 0 ? 1 : 2);
+        const uint32_t ctx = (kSignTab >> (3 * (hc * 3 + vc))) & 7u;
+        t[k] = (uint8_t)((ctx >> 1) | ((ctx & 1u) << 2));
+    }
+}
+
 struct Params {
     const int32_t *in;   // encode: raster coefficients; decode: slot stream
     int32_t *out;        // encode: slot stream; decode: raster coefficients
@@ -253,8 +270,9 @@ struct Coder {
     W &w;
     const Params &p;
     Lane s;
-    uint32_t *ring;      // per codeblock (decoder)
-    const uint8_t *tab;  // LUT bytes
+    uint32_t *ring;        // per codeblock (decoder)
+    const uint8_t *tab;    // LUT bytes
+    const uint8_t *sgtab;  // decoder: sign-context table (build_sign_table)
     const int32_t *slot_in;
     int32_t *slot_out;
     uint32_t in_cap;  // decoder: words readable at slot_in (slot size, or the compact length)
@@ -278,9 +296,9 @@ struct Coder {
     // inside this struct would keep the whole struct out of registers)
     uint32_t (*planes)[4];
 
-    BPC_FI Coder(W &w_, const Params &p_, uint32_t *ring_all, const uint8_t *tab_, uint32_t (*planes_)[4],
-                 uint8_t *ev_key_, uint32_t *ev_val_)
-        : w(w_), p(p_), tab(tab_), planes(planes_), ev_key(ev_key_), ev_val(ev_val_) {
+    BPC_FI Coder(W &w_, const Params &p_, uint32_t *ring_all, const uint8_t *tab_, const uint8_t *sgtab_,
+                 uint32_t (*planes_)[4], uint8_t *ev_key_, uint32_t *ev_val_)
+        : w(w_), p(p_), tab(tab_), sgtab(sgtab_), planes(planes_), ev_key(ev_key_), ev_val(ev_val_) {
         evmask = ring_all;
         pfx = ring_all + 256;
         lane = w.lane();
@@ -432,20 +450,15 @@ struct Coder {
             B[1] |= bit1;
         }
         if (!w.any(ns)) return;
-        // sign call (Compute_Sign_Context :178-226 over u, l, r, b), the table
-        // as boolean functions of the sign-sum classes (see enc_sign_slices)
+        // sign call (Compute_Sign_Context :178-226 over l, r, u, b): one lookup
+        // in the sign-context table indexed by the neighbours' bits
         const uint64_t LN = c ? s.N[0] : s.XNL, MN = c ? s.N[1] : s.N[0], RN = c ? s.XNR : s.N[1];
-        const uint32_t sl = (wl >> 1) & 1u, sr = (wr >> 1) & 1u, su = wm & 1u, sb = (wm >> 2) & 1u;
         const uint32_t nl = bith<H>(LN, j), nr = bith<H>(RN, j), wmn = win3h<H>(MN, j);
-        const uint32_t nu = wmn & 1u, nb = (wmn >> 2) & 1u;
-        const uint32_t pl = sl & ~nl, ml = sl & nl, pr = sr & ~nr, mr = sr & nr;
-        const uint32_t pu = su & ~nu, mu = su & nu, pb = sb & ~nb, mb = sb & nb;
-        const uint32_t hp = (pl & ~mr) | (pr & ~ml), hn = (ml & ~pr) | (mr & ~pl);
-        const uint32_t vp = (pu & ~mb) | (pb & ~mu), vn = (mu & ~pb) | (mb & ~pu);
-        const uint32_t h0 = ~(hp | hn) & 1u, v0 = ~(vp | vn) & 1u;
-        const uint32_t sidx = ((h0 & ~v0) | (hp & vp) | (hn & vn)) | (((hp & ~vn) | (hn & ~vp)) << 1);
-        const uint32_t pred = (h0 & vn) | hn;
-        const uint32_t P2 = ns ? tab[sign_base + (int)(sidx & 3u)] : 0u;
+        const uint32_t sk = ((wl >> 1) & 1u) | (nl << 1) | ((wr & 2u) << 1) | (nr << 3) | ((wm & 1u) << 4) |
+                            ((wmn & 1u) << 5) | ((wm & 4u) << 4) | ((wmn & 4u) << 5);
+        const uint32_t se = sgtab[sk];
+        const uint32_t sidx = se & 3u, pred = se >> 2;
+        const uint32_t P2 = ns ? tab[sign_base + (int)sidx] : 0u;
         const uint32_t neg = (ac_dec(ns, P2) ^ pred) & 1u;
         if (ns && neg) {
             s.N[0] |= bit0;

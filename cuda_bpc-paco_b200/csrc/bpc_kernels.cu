@@ -61,17 +61,20 @@ __global__ void __launch_bounds__(kWarps * 32, ENC ? kMinCtasEnc : kMinCtasDec) 
         tab[k] = (uint8_t)v;
     }
     if (bad && p.status) atomicOr(p.status, ST_LUT_RANGE);
+    uint8_t *sgtab = smem + p.tab_n;
+    if (!ENC) build_sign_table(sgtab, (int)threadIdx.x, (int)blockDim.x);
     __syncthreads();
     const int warp = (int)(threadIdx.x >> 5);
     // per warp: the decoder's codeword ring, or the encoder's event ranking words
-    uint32_t *ring = reinterpret_cast<uint32_t *>(smem + p.tab_n) + warp * (ENC ? 512 : G::RING_WORDS);
+    uint32_t *ring =
+        reinterpret_cast<uint32_t *>(smem + p.tab_n + kSignTableBytes) + warp * (ENC ? 512 : G::RING_WORDS);
     GpuWarp w;
     uint32_t planes[28][4];  // per-thread bitplanes (local memory, L1-resident)
     uint8_t ev_key[ENC ? 256 : 1];
     uint32_t ev_val[ENC ? 256 : 1];
     const int stride = (int)gridDim.x * kWarps * G::NG;
     for (int base = p.cb_begin + ((int)blockIdx.x * kWarps + warp) * G::NG; base < p.cb_end; base += stride) {
-        Coder<PASSES, CBS, ENC, GpuWarp> cd(w, p, ring, tab, planes, ev_key, ev_val);
+        Coder<PASSES, CBS, ENC, GpuWarp> cd(w, p, ring, tab, sgtab, planes, ev_key, ev_val);
         cd.run(base);
     }
 }
@@ -89,7 +92,7 @@ __global__ void __launch_bounds__(kWarps * 32, kMinCtasEnc) k_bpc_stats(Params p
     uint32_t ev_val[1];
     const int stride = (int)gridDim.x * kWarps * G::NG;
     for (int base = p.cb_begin + ((int)blockIdx.x * kWarps + warp) * G::NG; base < p.cb_end; base += stride) {
-        Coder<PASSES, CBS, true, GpuWarp> cd(w, p, ring, nullptr, planes, ev_key, ev_val);
+        Coder<PASSES, CBS, true, GpuWarp> cd(w, p, ring, nullptr, nullptr, planes, ev_key, ev_val);
         cd.template run<true>(base, stats);
     }
 }
@@ -114,7 +117,7 @@ cudaError_t launch_stats(int passes, int cbs, const Params &p, unsigned long lon
 template <int PASSES, int CBS, bool ENC>
 static size_t smem_bytes(const Params &p) {
     using G = Geo<CBS>;
-    return (size_t)p.tab_n + (size_t)kWarps * 4u * (size_t)(ENC ? 512 : G::RING_WORDS);
+    return (size_t)p.tab_n + (size_t)kSignTableBytes + (size_t)kWarps * 4u * (size_t)(ENC ? 512 : G::RING_WORDS);
 }
 
 template <int PASSES, int CBS, bool ENC>
