@@ -431,6 +431,7 @@ struct Coder {
                 s.C[1] |= bit1;
                 coded = false;
             }
+            if (!w.any(coded)) return;  // every candidate deferred
         }
         const uint32_t P = coded ? tab[sig_base + popc32(nbh)] : 0u;
         const uint32_t sym = ac_dec(coded, P);
