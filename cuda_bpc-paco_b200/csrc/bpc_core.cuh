@@ -411,11 +411,13 @@ struct Coder {
     // number of reservations before it.  So the warp walks the steps that
     // have a candidate in some lane, all lanes together, and the rows are
     // visited per 32-row half so that every row access is a 32-bit shift.
-    // One step (row 32H + j, column c).  c is a run-time value so that the
-    // decoder has one step body per pass kind and half: warps in different
-    // passes share the instruction cache.
-    template <int PK, int H>
-    BPC_FI void dec_ctx_step(int j, int c, int b, bool act) {
+    // One step (row 32H + j, column c).  In 3-pass mode c is a run-time value
+    // so that the decoder has one step body per pass kind and half and warps
+    // in different passes share the instruction cache; 2-pass mode has half
+    // the bodies and takes c as a constant (no selects between the columns).
+    template <int PK, int H, int CC>
+    BPC_FI void dec_ctx_step(int j, int c_rt, int b, bool act) {
+        const int c = CC >= 0 ? CC : c_rt;
         const uint64_t S0 = s.S[0], S1 = s.S[1], Sc = c ? S1 : S0;
         const bool cand = act && (PK == PK_SPP ? !bith<H>(Sc, j) : bith<H>(c ? s.C[1] : s.C[0], j));
         if (!w.any(cand)) return;
@@ -488,8 +490,13 @@ struct Coder {
         while (u) {
             const int j = ctz64(u);
             u &= u - 1;
+            if constexpr (PASSES == 2) {
+                dec_ctx_step<PK, H, 0>(j, 0, b, act);
+                dec_ctx_step<PK, H, 1>(j, 1, b, act);
+            } else {
 #pragma unroll 1
-            for (int c = 0; c < 2; c++) dec_ctx_step<PK, H>(j, c, b, act);
+                for (int c = 0; c < 2; c++) dec_ctx_step<PK, H, -1>(j, c, b, act);
+            }
         }
     }
 
@@ -507,21 +514,28 @@ struct Coder {
 
     // MRP_Decoder :608-629
     template <int H>
+    BPC_FI void dec_mrp_step(int j, int c, int b, bool act, uint32_t P) {
+        const bool cand = act && bith<H>(c ? s.R[1] : s.R[0], j);
+        if (!w.any(cand)) return;
+        ring_ensure();
+        const uint32_t sym = ac_dec(cand, P);
+        if (cand && sym && b <= 27) {
+            const uint64_t bit = maskh<H>(1u, j);
+            B[0] |= c ? 0ull : bit;
+            B[1] |= c ? bit : 0ull;
+        }
+    }
+    template <int H>
     BPC_FI void dec_mrp_half(uint32_t u, int b, bool act, uint32_t P) {
         while (u) {
             const int j = ctz64(u);
             u &= u - 1;
+            if constexpr (PASSES == 2) {
+                dec_mrp_step<H>(j, 0, b, act, P);
+                dec_mrp_step<H>(j, 1, b, act, P);
+            } else {
 #pragma unroll 1
-            for (int c = 0; c < 2; c++) {
-                const bool cand = act && bith<H>(c ? s.R[1] : s.R[0], j);
-                if (!w.any(cand)) continue;
-                ring_ensure();
-                const uint32_t sym = ac_dec(cand, P);
-                if (cand && sym && b <= 27) {
-                    const uint64_t bit = maskh<H>(1u, j);
-                    B[0] |= c ? 0ull : bit;
-                    B[1] |= c ? bit : 0ull;
-                }
+                for (int c = 0; c < 2; c++) dec_mrp_step<H>(j, c, b, act, P);
             }
         }
     }
