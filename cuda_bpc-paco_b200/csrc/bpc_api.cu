@@ -30,7 +30,7 @@ struct DropInState {
     size_t cap = 0;
     // host-buffer calls run bands of codeblock rows on these streams so that
     // the copies in both directions overlap the kernels
-    static constexpr int kStreams = 3;
+    static constexpr int kStreams = 8;
     cudaStream_t streams[kStreams] = {};
     cudaEvent_t done[kStreams] = {};
 };
@@ -132,10 +132,13 @@ int code_host_locked(DropInState &s, int direction, int *hdata, int X, int Y, co
     // are contiguous in both layouts (coefficients row-major, slots in raster
     // order of codeblocks)
     const int ncbx = X / cb, rows = Y / cb;
-    // at least ~1024 codeblocks per band so that each band's kernel still fills the GPU
+    // bands of at least 512 codeblocks (each band's kernel still spreads over
+    // the SMs), at most 32 (shorter pipeline fill and drain on large images);
+    // bands go round-robin over the 8 streams, so a band's copy-in waits at
+    // most behind the band 8 places earlier
     const long long ncb = (long long)ncbx * rows;
-    int nband = (int)(ncb / 1024);
-    nband = nband < 1 ? 1 : (nband > 8 ? 8 : nband);
+    int nband = (int)(ncb / 512);
+    nband = nband < 1 ? 1 : (nband > 32 ? 32 : nband);
     if (nband > rows) nband = rows;
     const size_t row_words = (size_t)X * (size_t)cb;  // one codeblock row, either layout
     for (int k = 0; k < nband; k++) {
