@@ -31,8 +31,10 @@
 
 #if defined(__CUDACC__)
 #define BPC_FI __device__ __forceinline__
+#define BPC_NOINLINE __device__ __noinline__
 #else
 #define BPC_FI inline
+#define BPC_NOINLINE inline
 #endif
 
 namespace bpc {
@@ -247,6 +249,39 @@ struct Lane {
     int nev;
 };
 
+// Decoder codeword ring refill: lane gl of a codeblock's lane group copies
+// its share of slot words [first, first + nwords) into the ring with 16-byte
+// loads; words past in_cap read as -1.  Kept out of line: it runs once per 256
+// codewords, and inlined into every decoder step body it would crowd the
+// instruction cache.
+template <int CBS>
+BPC_NOINLINE void ring_fill(uint32_t *ring, const int32_t *slot_in, uint32_t in_cap, bool compact, uint32_t first,
+                            int gl, int nwords) {
+    constexpr int NL = CBS / 2, RING = CBS == 64 ? 512 : 256;
+    const int per = nwords / NL;  // 8 or 16, multiple of 4
+    for (int q = 0; q < per; q += 4) {
+        const uint32_t k = first + (uint32_t)(gl * per + q);
+        uint32_t v0, v1, v2, v3;
+        if (k + 3 < in_cap && !compact) {
+            const int4 v = *reinterpret_cast<const int4 *>(slot_in + k);
+            v0 = (uint32_t)v.x;
+            v1 = (uint32_t)v.y;
+            v2 = (uint32_t)v.z;
+            v3 = (uint32_t)v.w;
+        } else {  // slot end, or the compact container (no 16-byte alignment)
+            v0 = k + 0 < in_cap ? (uint32_t)slot_in[k + 0] : 0xFFFFFFFFu;
+            v1 = k + 1 < in_cap ? (uint32_t)slot_in[k + 1] : 0xFFFFFFFFu;
+            v2 = k + 2 < in_cap ? (uint32_t)slot_in[k + 2] : 0xFFFFFFFFu;
+            v3 = k + 3 < in_cap ? (uint32_t)slot_in[k + 3] : 0xFFFFFFFFu;
+        }
+        const uint32_t r = k & (RING - 1);
+        ring[r] = v0;
+        ring[r + 1] = v1;
+        ring[r + 2] = v2;
+        ring[r + 3] = v3;
+    }
+}
+
 template <class W>
 BPC_FI uint64_t warp_or64(W &w, uint64_t v) {
     return ((uint64_t)w.reduce_or((uint32_t)(v >> 32)) << 32) | w.reduce_or((uint32_t)v);
@@ -346,25 +381,7 @@ struct Coder {
 
     // decoder: make sure ring holds slot words [cnt+1, cnt+1+2*NL)
     BPC_FI void ring_load(uint32_t first, int nwords) {
-        // group-cooperative, 16-byte loads; words past the slot read as -1
-        const int per = nwords / G::NL;  // 8 or 16, multiple of 4
-        for (int q = 0; q < per; q += 4) {
-            const uint32_t k = first + (uint32_t)(gl * per + q);
-            uint32_t v0, v1, v2, v3;
-            if (k + 3 < in_cap && p.offsets == nullptr) {
-                w.load4(slot_in + k, v0, v1, v2, v3);
-            } else {  // slot end, or the compact container (no 16-byte alignment)
-                v0 = k + 0 < in_cap ? (uint32_t)slot_in[k + 0] : 0xFFFFFFFFu;
-                v1 = k + 1 < in_cap ? (uint32_t)slot_in[k + 1] : 0xFFFFFFFFu;
-                v2 = k + 2 < in_cap ? (uint32_t)slot_in[k + 2] : 0xFFFFFFFFu;
-                v3 = k + 3 < in_cap ? (uint32_t)slot_in[k + 3] : 0xFFFFFFFFu;
-            }
-            const uint32_t r = k & (G::RING - 1);
-            ring[r] = v0;
-            ring[r + 1] = v1;
-            ring[r + 2] = v2;
-            ring[r + 3] = v3;
-        }
+        ring_fill<CBS>(ring, slot_in, in_cap, p.offsets != nullptr, first, gl, nwords);
     }
     BPC_FI void ring_ensure() {
         if (s.cnt + 1u + 2u * G::NL > s.ring_hi) {  // group-uniform
@@ -411,10 +428,9 @@ struct Coder {
     // number of reservations before it.  So the warp walks the steps that
     // have a candidate in some lane, all lanes together, and the rows are
     // visited per 32-row half so that every row access is a 32-bit shift.
-    // One step (row 32H + j, column c).  In 3-pass mode c is a run-time value
-    // so that the decoder has one step body per pass kind and half and warps
-    // in different passes share the instruction cache; 2-pass mode has half
-    // the bodies and takes c as a constant (no selects between the columns).
+    // One step (row 32H + j, column c), with c a constant: no selects between
+    // the columns.  The step bodies (pass kind x half x column) fit the
+    // instruction cache because the rare codeword-ring refill is out of line.
     template <int PK, int H, int CC>
     BPC_FI void dec_ctx_step(int j, int c_rt, int b, bool act) {
         const int c = CC >= 0 ? CC : c_rt;
@@ -490,13 +506,8 @@ struct Coder {
         while (u) {
             const int j = ctz64(u);
             u &= u - 1;
-            if constexpr (PASSES == 2) {
-                dec_ctx_step<PK, H, 0>(j, 0, b, act);
-                dec_ctx_step<PK, H, 1>(j, 1, b, act);
-            } else {
-#pragma unroll 1
-                for (int c = 0; c < 2; c++) dec_ctx_step<PK, H, -1>(j, c, b, act);
-            }
+            dec_ctx_step<PK, H, 0>(j, 0, b, act);
+            dec_ctx_step<PK, H, 1>(j, 1, b, act);
         }
     }
 
