@@ -383,8 +383,12 @@ struct Coder {
     BPC_FI void ring_load(uint32_t first, int nwords) {
         ring_fill<CBS>(ring, slot_in, in_cap, p.offsets != nullptr, first, gl, nwords);
     }
+    // CALLS = AC calls before the next check (each reserves at most NL
+    // codewords); a refill of CHUNK words keeps [cnt+1, cnt+1+CALLS*NL) in the
+    // ring for CALLS <= 4
+    template <int CALLS>
     BPC_FI void ring_ensure() {
-        if (s.cnt + 1u + 2u * G::NL > s.ring_hi) {  // group-uniform
+        if (s.cnt + 1u + (uint32_t)(CALLS * G::NL) > s.ring_hi) {  // group-uniform
             w.syncmask(gmask);
             ring_load(s.ring_hi, G::CHUNK);
             s.ring_hi += G::CHUNK;
@@ -437,7 +441,6 @@ struct Coder {
         const uint64_t S0 = s.S[0], S1 = s.S[1], Sc = c ? S1 : S0;
         const bool cand = act && (PK == PK_SPP ? !bith<H>(Sc, j) : bith<H>(c ? s.C[1] : s.C[0], j));
         if (!w.any(cand)) return;
-        ring_ensure();
         const uint64_t Lm = c ? S0 : s.XL, Rm = c ? s.XR : S1;
         const uint32_t wl = win3h<H>(Lm, j), wm = win3h<H>(Sc, j), wr = win3h<H>(Rm, j);
         const uint32_t nbh = wl | ((wm & 5u) << 3) | (wr << 6);
@@ -506,6 +509,7 @@ struct Coder {
         while (u) {
             const int j = ctz64(u);
             u &= u - 1;
+            ring_ensure<4>();  // one row: two steps of up to two AC calls
             dec_ctx_step<PK, H, 0>(j, 0, b, act);
             dec_ctx_step<PK, H, 1>(j, 1, b, act);
         }
@@ -528,7 +532,6 @@ struct Coder {
     BPC_FI void dec_mrp_step(int j, int c, int b, bool act, uint32_t P) {
         const bool cand = act && bith<H>(c ? s.R[1] : s.R[0], j);
         if (!w.any(cand)) return;
-        ring_ensure();
         const uint32_t sym = ac_dec(cand, P);
         if (cand && sym && b <= 27) {
             const uint64_t bit = maskh<H>(1u, j);
@@ -541,6 +544,7 @@ struct Coder {
         while (u) {
             const int j = ctz64(u);
             u &= u - 1;
+            ring_ensure<2>();  // one row: two steps of one AC call
             if constexpr (PASSES == 2) {
                 dec_mrp_step<H>(j, 0, b, act, P);
                 dec_mrp_step<H>(j, 1, b, act, P);
