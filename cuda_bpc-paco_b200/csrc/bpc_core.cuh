@@ -489,8 +489,7 @@ struct Coder {
         // neighbour columns: lane l's column c at row i changed; lane l-1
         // (column 0) or lane l+1 (column 1) takes it over with one shuffle
         const uint32_t mine = ns ? (1u | (neg << 1)) : 0u;
-        const int src = c ? lane - 1 : lane + 1;
-        const uint32_t got = w.shfl_idx(mine, src & 31);
+        const uint32_t got = c ? w.shfl_up(mine, 1) : w.shfl_down(mine, 1);
         if (c == 0) {
             if (gl < G::NL - 1) {
                 s.XR |= maskh<H>(got & 1u, j);
