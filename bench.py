@@ -639,13 +639,125 @@ def run_ours(args, c):
         print(json.dumps(line))
 
 
+def _timed(fn, stream, flush, steps, warmup):
+    """Median device time (s) of fn() over `steps` runs after `warmup`, each
+    preceded by an L2 flush, CUDA events on `stream`."""
+    import torch
+    ts = []
+    for k in range(warmup + steps):
+        flush.fill_(k & 255)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        if k >= warmup:
+            ts.append(e0.elapsed_time(e1) / 1e3)
+    return float(np.median(ts))
+
+
+def run_dwt(args):
+    """The GPU 5/3 DWT (bpc_dwt53_forward / _inverse) on cfg5's 16384x16384
+    image, 5 levels.  Algorithmic bytes: every level reads and writes its
+    region once for the row step and once for the column step (16 B per
+    coefficient of the level), so 16 B x N x sum 4^-l per direction."""
+    import torch
+    import bpc_paco as bpc
+    import bpc_synth
+    c = CONFIGS["cfg5"]
+    side, levels = c["side"], c["levels"]
+    N = side * side
+    img = bpc_synth.make_image_gpu(side, 1, c["amp"], c["nrect"]) - 128
+    ref = img.clone()
+    tmp = torch.empty_like(img)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    stream = torch.cuda.current_stream()
+    fwd = ref.clone()
+    bpc.dwt53(fwd, levels, tmp=tmp)
+    # each timed call transforms a fresh copy of its input; the copy is timed
+    # alone and subtracted
+    w = max(args.warmup, 3)
+    tc = _timed(lambda: img.copy_(ref), stream, flush, args.steps, w)
+    tf = _timed(lambda: (img.copy_(ref), bpc.dwt53(img, levels, tmp=tmp)), stream, flush, args.steps, w) - tc
+    assert torch.equal(img, fwd), "forward differs between runs"
+    ti = _timed(lambda: (img.copy_(fwd), bpc.dwt53(img, levels, inverse=True, tmp=tmp)), stream, flush, args.steps,
+                w) - tc
+    assert torch.equal(img, ref), "inverse(forward(x)) != x"
+    alg = 16.0 * N * sum(4.0 ** -l for l in range(levels))
+    peak, peak_kind = load_peaks()
+    # e2e: pinned host image -> device, forward, -> host; and back through the inverse
+    h = torch.empty(N, dtype=torch.int32, pin_memory=True)
+    h.copy_(ref.view(-1))
+    d = torch.empty_like(img)
+    te = []
+    for k in range(max(args.warmup, 3) + min(args.steps, 20)):
+        t0 = time.perf_counter()
+        d.view(-1).copy_(h, non_blocking=True)
+        bpc.dwt53(d, levels, tmp=tmp)
+        h.copy_(d.view(-1), non_blocking=True)
+        d.view(-1).copy_(h, non_blocking=True)
+        bpc.dwt53(d, levels, inverse=True, tmp=tmp)
+        h.copy_(d.view(-1), non_blocking=True)
+        torch.cuda.synchronize()
+        if k >= max(args.warmup, 3):
+            te.append(time.perf_counter() - t0)
+    assert torch.equal(h.cuda().view(side, side), ref)
+    line = {
+        "metric": "5/3 DWT forward+inverse Gcoeff/s (lossless)", "value": 2 * N / (tf + ti) / 1e9,
+        "unit": "Gcoeff/s", "n_gpus": 1, "steps": args.steps, "warmup": max(args.warmup, 3),
+        "ms_per_step": 1e3 * (tf + ti), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "int32", "data": "synthetic (GPU generator)",
+        "config": {"workload": f"{side}x{side} image, {levels}-level reversible CDF 5/3 DWT, forward then inverse",
+                   "l2": "flushed (256 MiB write) before every timed call"},
+        "forward_ms": 1e3 * tf, "inverse_ms": 1e3 * ti,
+        "e2e": {"value": 2 * N / float(np.median(te)) / 1e9, "unit": "Gcoeff/s", "h2d_bytes_per_step": 8 * N,
+                "d2h_bytes_per_step": 8 * N},
+        "gpu_launches": "per level: 4 forward / 4 inverse kernels",
+        "roofline": {"bound": "hbm", "achieved": alg / max(tf, ti) / 1e9, "peak": peak, "unit": "GB/s",
+                     "frac": alg / max(tf, ti) / 1e9 / peak, "traffic": None, "peak_source": peak_kind,
+                     "note": "16 B per coefficient and level (row step + column step, read + write)"},
+    }
+    print(json.dumps(line))
+
+
+def run_train(args):
+    """LUT training statistics (bpc_lut_stats) on the cfg2 image: the
+    encoder's mask stage without its coder.  Algorithmic bytes: 4 B per
+    coefficient read."""
+    import torch
+    import bpc_paco as bpc
+    c = CONFIGS["cfg2"]
+    img = make_input(c, 1)
+    N = img.size
+    d = torch.from_numpy(img).cuda()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    stream = torch.cuda.current_stream()
+    st = bpc.lut_stats(d, c["passes"], c["levels"], c["cb"])
+    torch.cuda.synchronize()
+    t = _timed(lambda: bpc.lut_stats(d, c["passes"], c["levels"], c["cb"], stats=st), stream, flush, args.steps,
+               max(args.warmup, 3))
+    n = st.cpu().numpy()
+    peak, peak_kind = load_peaks()
+    line = {
+        "metric": "LUT training statistics Gcoeff/s", "value": N / t / 1e9, "unit": "Gcoeff/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": 1e3 * t, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded generator + 5/3 DWT)",
+        "config": {"workload": workload_name(c) + ", symbol counts per LUT entry", "l2": "flushed before every call"},
+        "symbols_counted_per_image": int(n[0::2].sum() // (args.steps + max(args.warmup, 3) + 1)),
+        "gpu_launches": 1,
+        "roofline": {"bound": "hbm", "achieved": 4.0 * N / t / 1e9, "peak": peak, "unit": "GB/s",
+                     "frac": 4.0 * N / t / 1e9 / peak, "traffic": None, "peak_source": peak_kind},
+    }
+    print(json.dumps(line))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="cfg2", choices=sorted(CONFIGS) + ["cfg3", "cfg4"])
+    ap.add_argument("--config", default="cfg2", choices=sorted(CONFIGS) + ["cfg3", "cfg4", "dwt", "train"])
     ap.add_argument("--images", type=int, default=192, help="cfg3: images per batch")
     ap.add_argument("--requests", type=int, default=20000, help="cfg4: requests per load level")
     ap.add_argument("--loads", type=float, nargs="+", default=[0.2, 0.5, 0.8, 1.0], help="cfg4: offered loads")
@@ -654,7 +766,10 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="kernel timing only (profiling runs)")
     args = ap.parse_args()
-    if args.config in ("cfg3", "cfg4"):
+    if args.config in ("dwt", "train") and args.impl == "ours":
+        (run_dwt if args.config == "dwt" else run_train)(args)
+        return
+    if args.config in ("cfg3", "cfg4", "dwt", "train"):
         if args.impl == "ours":
             (run_batched if args.config == "cfg3" else run_served)(args)
             return

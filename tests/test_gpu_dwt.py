@@ -8,7 +8,8 @@ import bpc_synth
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("H,W,levels", [(256, 256, 5), (384, 256, 4), (512, 1024, 6), (64, 64, 1)])
+@pytest.mark.parametrize("H,W,levels", [(256, 256, 5), (384, 256, 4), (512, 1024, 6), (64, 64, 1), (16, 16, 4),
+                                         (24, 40, 2), (8, 2048, 3)])
 def test_dwt_matches_numpy(bpc, H, W, levels):
     import torch
     rng = np.random.default_rng(H * W + levels)
