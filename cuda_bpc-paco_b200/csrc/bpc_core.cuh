@@ -580,8 +580,7 @@ struct Coder {
     // predicates the call so that the optional sign call needs no branch.
     BPC_FI void enc_symbol_if(bool on, uint32_t sym, uint32_t P, int key) {
         if (on && s.size == 0) {
-            ev_key[s.nev] = (uint8_t)key;
-            ev_val[s.nev] = 0u;
+            ev_key[s.nev] = (uint8_t)key;  // its value is stored when the codeword completes
             s.cur_ev = s.nev;
             s.nev++;
             w.smem_or(&evmask[key], 1u << lane);
@@ -601,34 +600,6 @@ struct Coder {
                 ev_val[s.cur_ev] = nlow;
             else if (s.open_slot < G::CAP)
                 slot_out[s.open_slot] = (int32_t)nlow;
-            else
-                s.status |= ST_OVERFLOW;
-        }
-    }
-
-    BPC_FI void enc_symbol(uint32_t sym, uint32_t P, int key) {
-        if (s.size == 0) {
-            ev_key[s.nev] = (uint8_t)key;
-            ev_val[s.nev] = 0u;
-            s.cur_ev = s.nev;
-            s.nev++;
-            w.smem_or(&evmask[key], 1u << lane);
-            s.has_resv = 1;
-            s.lower = 0;
-            s.size = 0xFFFFu;
-        }
-        const uint32_t t = ((s.size * P) >> 7) + sym;
-        if (sym) {
-            s.size -= t;
-            s.lower += t;
-        } else {
-            s.size = t;
-        }
-        if (s.size == 0) {
-            if (s.cur_ev >= 0)
-                ev_val[s.cur_ev] = s.lower;
-            else if (s.open_slot < G::CAP)
-                slot_out[s.open_slot] = (int32_t)s.lower;
             else
                 s.status |= ST_OVERFLOW;
         }
