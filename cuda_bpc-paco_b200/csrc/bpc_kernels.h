@@ -16,7 +16,10 @@ constexpr int kWarps = 4;  // warps (codeblocks) per CTA
 // together and needs many warps to hide latency (7 x 4 warps, <= 72
 // registers); the encoder runs each lane's coder on its own and needs the
 // registers more than the warps.
-constexpr int kMinCtasDec = 7;
+#ifndef DEC_MIN_CTAS
+#define DEC_MIN_CTAS 7
+#endif
+constexpr int kMinCtasDec = DEC_MIN_CTAS;
 constexpr int kMinCtasEnc = ENC_MIN_CTAS;
 
 // Launch the encoder (enc) or decoder over p.ncb codeblocks.  grid <= 0 picks
