@@ -150,13 +150,20 @@ def cpu_baseline(img, lut_np, c, budget_s=12.0):
     oracle.decode(s, img.shape, lut_np, c["passes"], c["levels"], c["cb"], threads, cb_range=(0, n))
     dt = time.perf_counter() - t0
     n2 = int(min(ncb, max(n, n * budget_s / max(dt, 1e-3))))
+    # the whole image may take less than the budget: code it repeatedly
+    reps = 0
     t0 = time.perf_counter()
-    s = oracle.encode(img, lut_np, c["passes"], c["levels"], c["cb"], threads, cb_range=(0, n2))
-    oracle.decode(s, img.shape, lut_np, c["passes"], c["levels"], c["cb"], threads, cb_range=(0, n2))
-    dt = time.perf_counter() - t0
-    coefs = n2 * c["cb"] * c["cb"]
+    while True:
+        s = oracle.encode(img, lut_np, c["passes"], c["levels"], c["cb"], threads, cb_range=(0, n2))
+        oracle.decode(s, img.shape, lut_np, c["passes"], c["levels"], c["cb"], threads, cb_range=(0, n2))
+        reps += 1
+        dt = time.perf_counter() - t0
+        if n2 < ncb or dt >= budget_s:
+            break
+    coefs = reps * n2 * c["cb"] * c["cb"]
+    what = f"the whole image x{reps}" if n2 == ncb else f"first {n2} of {ncb} codeblocks of the same image"
     return {"value": 2 * coefs / dt / 1e9, "unit": "Gcoeff/s", "cores": threads, "kind": "port",
-            "sample": f"first {n2} of {ncb} codeblocks of the same image, encode+decode, {dt:.1f} s"}
+            "sample": f"{what}, encode+decode, {dt:.1f} s"}
 
 
 def make_input(c, seed):
