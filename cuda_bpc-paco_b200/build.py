@@ -18,7 +18,7 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libbpc_paco.so")
 SOURCES = ["bpc_kernels.cu", "bpc_api.cu", "bpc_batch.cu", "bpc_noalloc.cu", "bpc_dwt.cu", "bpc_server.cu",
            "bpc_train.cu", "bpc_lut.cpp", "bpc_files.cpp"]
-HEADERS = ["bpc_core.cuh", "bpc_kernels.h", "bpc_lut.h"]
+HEADERS = ["bpc_core.cuh", "bpc_kernels.h", "bpc_lut.h", "bpc_arena.h"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O2", "-shared", "-Xptxas", "-O3"]

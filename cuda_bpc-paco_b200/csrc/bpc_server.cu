@@ -40,53 +40,11 @@
 #include <vector>
 
 #include "../../include/bpc_paco.h"
+#include "bpc_arena.h"
 
 namespace {
 
 using Clock = std::chrono::steady_clock;
-
-// first-fit allocator over the address-ordered free ranges of the arena
-class Arena {
-   public:
-    void init(size_t n) {
-        free_.clear();
-        free_[0] = n;
-        used_ = 0;
-    }
-    bool alloc(size_t n, size_t *off) {
-        for (auto it = free_.begin(); it != free_.end(); ++it) {
-            if (it->second < n) continue;
-            *off = it->first;
-            const size_t rest = it->second - n, at = it->first + n;
-            free_.erase(it);
-            if (rest) free_[at] = rest;
-            used_ += n;
-            return true;
-        }
-        return false;
-    }
-    void release(size_t off, size_t n) {
-        used_ -= n;
-        auto nx = free_.lower_bound(off);
-        if (nx != free_.end() && off + n == nx->first) {  // merge with the next range
-            n += nx->second;
-            nx = free_.erase(nx);
-        }
-        if (nx != free_.begin()) {  // merge with the previous range
-            auto pv = std::prev(nx);
-            if (pv->first + pv->second == off) {
-                pv->second += n;
-                return;
-            }
-        }
-        free_[off] = n;
-    }
-    size_t used() const { return used_; }
-
-   private:
-    std::map<size_t, size_t> free_;
-    size_t used_ = 0;
-};
 
 struct Lut {
     const int *d;
@@ -129,7 +87,7 @@ struct Server {
     int device = 0;
     unsigned char *base = nullptr;
     size_t budget = 0;
-    Arena arena;
+    bpc::Arena arena;
     std::vector<Lut> luts;
     std::deque<Request> queue;
     std::vector<Slot> slots;
