@@ -25,7 +25,9 @@
 // warps fits 7 times per SM.  The LUT sits in shared memory as bytes.
 //
 // The code is written against a small warp interface W (lane id, ballot, any,
-// shuffles, syncwarp) so the same source runs as a CUDA kernel (bpc_kernels.cu).
+// shuffles, syncwarp) so the same source runs as a CUDA kernel (bpc_kernels.cu)
+// and, compiled for the host with one thread per lane, in the CPU tests
+// (tests/emu/emu_warp.cpp).
 #pragma once
 #include <stdint.h>
 
@@ -263,11 +265,18 @@ BPC_NOINLINE void ring_fill(uint32_t *ring, const int32_t *slot_in, uint32_t in_
         const uint32_t k = first + (uint32_t)(gl * per + q);
         uint32_t v0, v1, v2, v3;
         if (k + 3 < in_cap && !compact) {
+#if defined(__CUDA_ARCH__)
             const int4 v = *reinterpret_cast<const int4 *>(slot_in + k);
             v0 = (uint32_t)v.x;
             v1 = (uint32_t)v.y;
             v2 = (uint32_t)v.z;
             v3 = (uint32_t)v.w;
+#else
+            v0 = (uint32_t)slot_in[k];
+            v1 = (uint32_t)slot_in[k + 1];
+            v2 = (uint32_t)slot_in[k + 2];
+            v3 = (uint32_t)slot_in[k + 3];
+#endif
         } else {  // slot end, or the compact container (no 16-byte alignment)
             v0 = k + 0 < in_cap ? (uint32_t)slot_in[k + 0] : 0xFFFFFFFFu;
             v1 = k + 1 < in_cap ? (uint32_t)slot_in[k + 1] : 0xFFFFFFFFu;

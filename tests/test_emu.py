@@ -1,0 +1,84 @@
+"""The product's coder source (cuda_bpc-paco_b200/csrc/bpc_core.cuh) compiled for
+the host and run with one user-level context per lane (tests/emu/emu_warp.cpp),
+checked bit-exact against the oracle: streams, decodes, status bits and LUT
+statistics.  No GPU; the same source the sm_100a kernels are built from."""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import bpc_synth
+from conftest import ROOT, lut_folder
+
+
+@pytest.fixture(scope="module")
+def emu(tmp_path_factory):
+    out = str(tmp_path_factory.mktemp("emu") / "libemu.so")
+    subprocess.check_call(["g++", "-O2", "-std=c++17", "-shared", "-fPIC", "-I",
+                           os.path.join(ROOT, "cuda_bpc-paco_b200", "csrc"),
+                           os.path.join(ROOT, "tests", "emu", "emu_warp.cpp"), "-o", out])
+    L = ctypes.CDLL(out)
+    vp = ctypes.c_void_p
+    L.emu_code.argtypes = [ctypes.c_int] * 4 + [vp, vp, ctypes.c_int, ctypes.c_int, vp, ctypes.c_int, ctypes.c_int,
+                                                  vp]
+    L.emu_code.restype = ctypes.c_int
+    return L
+
+
+def run(emu, enc, img_or_stream, shape, lut, passes, levels, cb, kind=0, stats=None):
+    Y, X = shape
+    src = np.ascontiguousarray(img_or_stream, dtype=np.int32).reshape(-1)
+    out = np.zeros(X * Y, np.int32)
+    rc = emu.emu_code(enc, kind, passes, cb, src.ctypes.data, out.ctypes.data, X, Y, lut.ctypes.data, lut.size,
+                      levels, None if stats is None else stats.ctypes.data)
+    assert rc >= 0, "lanes of a warp met different collectives"
+    return out, rc
+
+
+def roundtrip(emu, oracle_mod, img, passes, levels, cb):
+    lut = oracle_mod.load_luts(lut_folder(passes), passes, levels)
+    want, wst = oracle_mod.encode(img, lut, passes, levels, cb, with_status=True)
+    got, st = run(emu, 1, img, img.shape, lut, passes, levels, cb)
+    np.testing.assert_array_equal(got, want)
+    assert st == int(np.bitwise_or.reduce(wst))
+    dec, _ = run(emu, 0, got, img.shape, lut, passes, levels, cb)
+    np.testing.assert_array_equal(dec.reshape(img.shape), oracle_mod.decode(want, img.shape, lut, passes, levels, cb))
+    return st
+
+
+@pytest.mark.parametrize("passes", [2, 3])
+@pytest.mark.parametrize("cb", [64, 32])
+def test_synthetic(emu, oracle_mod, passes, cb):
+    img = bpc_synth.synthetic_coefficients(256, 5, 3, amp=40)
+    assert roundtrip(emu, oracle_mod, img, passes, 5, cb) == 0
+
+
+@pytest.mark.parametrize("passes", [2, 3])
+def test_straddling_and_sparse(emu, oracle_mod, passes):
+    img = np.ascontiguousarray(bpc_synth.synthetic_coefficients(3072, 5, 21, amp=30)[:64, :384])
+    roundtrip(emu, oracle_mod, img, passes, 5, 64)
+    z = np.zeros((128, 128), np.int32)
+    z[70, 3] = -1
+    z[127, 127] = 1 << 20
+    roundtrip(emu, oracle_mod, z, passes, 5, 64)
+
+
+def test_plane15_and_overflow(emu, oracle_mod):
+    img = bpc_synth.laplacian_coefficients(128, 5, 4)
+    img[0, 0] = 40000
+    roundtrip(emu, oracle_mod, img, 3, 5, 64)
+    rng = np.random.default_rng(3)
+    noisy = rng.integers(-(1 << 15), 1 << 15, size=(64, 64)).astype(np.int32)
+    assert roundtrip(emu, oracle_mod, noisy, 2, 5, 64) & 1  # slot overflow, dropped like the oracle
+
+
+@pytest.mark.parametrize("passes,cb", [(3, 64), (2, 32)])
+def test_lut_statistics(emu, oracle_mod, passes, cb):
+    img = bpc_synth.synthetic_coefficients(128, 5, 12, amp=30)
+    lut = oracle_mod.load_luts(lut_folder(passes), passes, 5)
+    n = oracle_mod.lut_entries(passes, 5)
+    st = np.zeros(2 * n, np.uint64)
+    run(emu, 1, img, img.shape, lut, passes, 5, cb, kind=1, stats=st)
+    np.testing.assert_array_equal(st, oracle_mod.lut_stats(img, passes, 5, cb))
