@@ -176,10 +176,12 @@ int run_all(const bpc::Params &p, const uint8_t *tab, const uint8_t *sgtab, unsi
 }  // namespace
 
 // enc = 1 encode (kind 0: slot stream, kind 1: LUT statistics into stats),
-// enc = 0 decode.  Returns the OR of the status bits, or -1 if the lanes of a
+// enc = 0 decode (of the slot stream, or of the compact container when
+// offsets is not null).  Returns the OR of the status bits, or -1 if the lanes of a
 // warp ever met different collectives.
 extern "C" int emu_code(int enc, int kind, int passes, int cbs, const int32_t *in, int32_t *out, int X, int Y,
-                        const int32_t *lut, int lut_n, int levels, unsigned long long *stats) {
+                        const int32_t *lut, int lut_n, int levels, unsigned long long *stats,
+                        const long long *offsets) {
     Sched sched;
     for (int l = 0; l < 32; l++) sched.stack[l].assign(kStack, 0);
     S = &sched;
@@ -208,7 +210,7 @@ extern "C" int emu_code(int enc, int kind, int passes, int cbs, const int32_t *i
     p.cp_off = o.cp_off;
     p.status = &status;
     p.counts = nullptr;
-    p.offsets = nullptr;
+    p.offsets = enc ? nullptr : offsets;  // decode from the compact container when given
     p.cb_begin = 0;
     p.cb_end = p.ncb;
     int rc;

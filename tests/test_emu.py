@@ -22,17 +22,18 @@ def emu(tmp_path_factory):
     L = ctypes.CDLL(out)
     vp = ctypes.c_void_p
     L.emu_code.argtypes = [ctypes.c_int] * 4 + [vp, vp, ctypes.c_int, ctypes.c_int, vp, ctypes.c_int, ctypes.c_int,
-                                                  vp]
+                                                  vp, vp]
     L.emu_code.restype = ctypes.c_int
     return L
 
 
-def run(emu, enc, img_or_stream, shape, lut, passes, levels, cb, kind=0, stats=None):
+def run(emu, enc, img_or_stream, shape, lut, passes, levels, cb, kind=0, stats=None, offsets=None):
     Y, X = shape
     src = np.ascontiguousarray(img_or_stream, dtype=np.int32).reshape(-1)
     out = np.zeros(X * Y, np.int32)
     rc = emu.emu_code(enc, kind, passes, cb, src.ctypes.data, out.ctypes.data, X, Y, lut.ctypes.data, lut.size,
-                      levels, None if stats is None else stats.ctypes.data)
+                      levels, None if stats is None else stats.ctypes.data,
+                      None if offsets is None else offsets.ctypes.data)
     assert rc >= 0, "lanes of a warp met different collectives"
     return out, rc
 
@@ -82,3 +83,20 @@ def test_lut_statistics(emu, oracle_mod, passes, cb):
     st = np.zeros(2 * n, np.uint64)
     run(emu, 1, img, img.shape, lut, passes, 5, cb, kind=1, stats=st)
     np.testing.assert_array_equal(st, oracle_mod.lut_stats(img, passes, 5, cb))
+
+
+@pytest.mark.parametrize("passes,cb", [(3, 64), (2, 32)])
+def test_decode_from_compact_container(emu, oracle_mod, passes, cb):
+    """The batched form's container (MSB + codewords per codeblock, int64
+    offsets, words past a codeblock read as the -1 fill) decodes like the slot
+    stream."""
+    img = bpc_synth.synthetic_coefficients(128, 5, 13, amp=30)
+    lut = oracle_mod.load_luts(lut_folder(passes), passes, 5)
+    slots = oracle_mod.encode(img, lut, passes, 5, cb).reshape(-1, cb * cb)
+    sizes = np.minimum((slots[:, 1:] != -1).sum(1) + 1, cb * cb)
+    offsets = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int64)
+    compact = np.concatenate([slots[g, :sizes[g]] for g in range(len(sizes))]).astype(np.int32)
+    buf = np.zeros(img.size, np.int32)
+    buf[:compact.size] = compact
+    dec, _ = run(emu, 0, buf, img.shape, lut, passes, 5, cb, offsets=offsets)
+    np.testing.assert_array_equal(dec.reshape(img.shape), img)
