@@ -553,13 +553,8 @@ struct Coder {
             const int j = ctz64(u);
             u &= u - 1;
             ring_ensure<2>();  // one row: two steps of one AC call
-            if constexpr (PASSES == 2) {
-                dec_mrp_step<H>(j, 0, b, act, P);
-                dec_mrp_step<H>(j, 1, b, act, P);
-            } else {
-#pragma unroll 1
-                for (int c = 0; c < 2; c++) dec_mrp_step<H>(j, c, b, act, P);
-            }
+            dec_mrp_step<H>(j, 0, b, act, P);
+            dec_mrp_step<H>(j, 1, b, act, P);
         }
     }
 
