@@ -361,13 +361,10 @@ struct Coder {
         if (ball) {  // warp-uniform
             const uint32_t bal = ball & gmask;
             if (need) {
+                // past the slot the ring holds the -1 fill; the overflow itself
+                // is reported once, from the final count, at the codeblock's end
                 const uint32_t idx = 1u + s.cnt + (uint32_t)popc32(bal & ltmask);
-                if (idx < (uint32_t)G::CAP) {
-                    s.cw = ring[idx & (G::RING - 1)];
-                } else {
-                    s.cw = 0xFFFFFFFFu;
-                    s.status |= ST_OVERFLOW;
-                }
+                s.cw = ring[idx & (G::RING - 1)];
                 s.lower = 0;
                 s.size = 0xFFFFu;
             }
@@ -1125,6 +1122,7 @@ struct Coder {
                 }
             }
         }
+        if (!ENC && ok && s.cnt >= (uint32_t)G::CAP) s.status |= ST_OVERFLOW;  // a reservation read past the slot
         if (ok && p.counts && gl == 0) p.counts[cb] = (int)s.cnt;
         int st = s.status;
         for (int o = 16; o; o >>= 1) st |= (int)w.shfl_xor((uint32_t)st, o);

@@ -44,8 +44,10 @@ def roundtrip(emu, oracle_mod, img, passes, levels, cb):
     got, st = run(emu, 1, img, img.shape, lut, passes, levels, cb)
     np.testing.assert_array_equal(got, want)
     assert st == int(np.bitwise_or.reduce(wst))
-    dec, _ = run(emu, 0, got, img.shape, lut, passes, levels, cb)
-    np.testing.assert_array_equal(dec.reshape(img.shape), oracle_mod.decode(want, img.shape, lut, passes, levels, cb))
+    dec, dst = run(emu, 0, got, img.shape, lut, passes, levels, cb)
+    wdec, wdst = oracle_mod.decode(want, img.shape, lut, passes, levels, cb, with_status=True)
+    np.testing.assert_array_equal(dec.reshape(img.shape), wdec)
+    assert dst == int(np.bitwise_or.reduce(wdst))
     return st
 
 

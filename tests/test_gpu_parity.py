@@ -25,8 +25,9 @@ def check_roundtrip(bpc, oracle_mod, img, passes, levels, cb, lut_np=None):
         assert bad.size == 0, f"first stream mismatch at {bad[:8]} (slot {bad[0] // (cb * cb)})"
         assert st == int(np.bitwise_or.reduce(wst))
         dec, dst = bpc.decode_host(got, img.shape, lut, cb)
-        wdec, _ = oracle_mod.decode(want, img.shape, lut_np, passes, levels, cb, with_status=True)
+        wdec, wdst = oracle_mod.decode(want, img.shape, lut_np, passes, levels, cb, with_status=True)
         np.testing.assert_array_equal(dec, wdec)
+        assert dst == int(np.bitwise_or.reduce(wdst))
         ok = np.nonzero(wst == 0)[0]
         ncbx = img.shape[1] // cb
         for k in ok[:: max(1, len(ok) // 64)]:
