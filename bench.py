@@ -48,7 +48,7 @@ CONFIGS = {
 METRIC = "encode/decode Gcoeff/s (bit-exact)"
 # DRAM read + write bytes of one launch of the dominant kernel (the decoder),
 # from the ncu capture summarised in profiles/k_bpc_cfg2_full.md.
-NCU_TRAFFIC = {"cfg2": 15.618816e6 + 20.613376e6}
+NCU_TRAFFIC = {"cfg2": 15.084288e6 + 18.242304e6}
 
 
 def workload_name(c):
