@@ -15,19 +15,21 @@
 // bits (:1120), every lane keeps its state as 64-bit column masks (bit i =
 // row i): significance S, refinement-eligible R, CP-pending C and sign N, plus
 // copies of the two neighbour columns (lane-1's right column, lane+1's left
-// column) that are kept current with one ballot per step that changes them.
-// A context is a popcount of a 9-bit neighbourhood gathered from three 3-row
-// windows; there are no per-coefficient shuffles.  Magnitudes are held as
-// bitplanes (one 64-bit row mask per plane and column) in a per-thread array
-// built with an in-register 32x32 bit transpose; the decoder collects decoded
-// planes the same way and transposes them back at the end.  No shared memory
-// is reserved per codeblock except the decoder's codeword ring, so a CTA of 4
-// warps fits 7 times per SM.  The LUT sits in shared memory as bytes.
+// column).  The encoder derives whole passes from these masks bit-parallel; the
+// decoder keeps the neighbour copies current with one shuffle per step in which
+// some lane's coefficient became significant.  A significance context is a
+// popcount of a 9-bit neighbourhood gathered from three 3-row windows, a sign
+// context one read of a 256-entry table.  Magnitudes are held as bitplanes (one
+// 64-bit row mask per plane and column) in a per-thread array built with an
+// in-register 32x32 bit transpose; the decoder collects decoded planes the same
+// way and transposes them back at the end.  Shared memory holds the LUT bytes,
+// the sign-context table and, per warp, the decoder's codeword ring or the
+// encoder's event-ranking words, so a decoder CTA of 4 warps fits 7 times per SM.
 //
 // The code is written against a small warp interface W (lane id, ballot, any,
 // shuffles, syncwarp) so the same source runs as a CUDA kernel (bpc_kernels.cu)
-// and, compiled for the host with one thread per lane, in the CPU tests
-// (tests/emu/emu_warp.cpp).
+// and, compiled for the host with one user-level context per lane, in the CPU
+// tests (tests/emu/emu_warp.cpp).
 #pragma once
 #include <stdint.h>
 
