@@ -59,7 +59,10 @@ def lib() -> ctypes.CDLL:
         L.bpc_encode_device.argtypes = dev
         L.bpc_decode_device.argtypes = dev
         L.bpc_lut_entries.argtypes = [ctypes.c_int] * 3
-        for f in ("bpc_set_mode", "bpc_get_mode", "bpc_last_status", "bpc_load_luts_host", "bpc_load_luts",
+        L.bpc_set_host_pipeline.argtypes = [ctypes.c_int] * 4
+        L.bpc_get_host_pipeline.argtypes = [ip, ip, ip, ip]
+        L.bpc_host_band_rows.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, vp, ctypes.c_int]
+        for f in ("bpc_set_host_pipeline", "bpc_get_host_pipeline", "bpc_host_band_rows", "bpc_set_mode", "bpc_get_mode", "bpc_last_status", "bpc_load_luts_host", "bpc_load_luts",
                   "bpc_lut_free", "bpc_code_host", "bpc_encode_device", "bpc_decode_device", "bpc_lut_entries",
                   "bpc_version"):
             getattr(L, f).restype = ctypes.c_int
@@ -90,6 +93,27 @@ def get_mode():
     a, b, c = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
     lib().bpc_get_mode(ctypes.byref(a), ctypes.byref(b), ctypes.byref(c))
     return a.value, b.value, c.value
+
+
+def set_host_pipeline(band_cbs: int, max_bands: int, streams: int, ramp: int = 0) -> None:
+    """Bands of >= band_cbs codeblocks, <= max_bands of them, on `streams` CUDA
+    streams for the host-buffer calls, the first and last `ramp` bands halving
+    towards the ends (speed only; outputs do not change)."""
+    _check(lib().bpc_set_host_pipeline(band_cbs, max_bands, streams, ramp), "bpc_set_host_pipeline")
+
+
+def get_host_pipeline():
+    v = [ctypes.c_int() for _ in range(4)]
+    lib().bpc_get_host_pipeline(*[ctypes.byref(x) for x in v])
+    return tuple(x.value for x in v)
+
+
+def host_band_rows(X: int, Y: int, cb: int = 64) -> list:
+    """First codeblock row of each band the host-buffer calls cut an X x Y image into."""
+    n = _check(lib().bpc_host_band_rows(X, Y, cb, None, 0), "bpc_host_band_rows")
+    buf = (ctypes.c_int * max(n, 1))()
+    lib().bpc_host_band_rows(X, Y, cb, buf, n)
+    return list(buf[:n])
 
 
 def load_LUTs(folder: str) -> int:

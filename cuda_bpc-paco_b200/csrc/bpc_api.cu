@@ -28,11 +28,14 @@ struct DropInState {
     // device buffers reused across CUDA_BPC calls (grow only)
     int *d_a = nullptr, *d_b = nullptr, *d_status = nullptr;
     size_t cap = 0;
-    // host-buffer calls run bands of codeblock rows on these streams so that
-    // the copies in both directions overlap the kernels
-    static constexpr int kStreams = 8;
-    cudaStream_t streams[kStreams] = {};
-    cudaEvent_t done[kStreams] = {};
+    // host-buffer calls run bands of codeblock rows round-robin on `nstreams`
+    // of these streams so that the copies in both directions overlap the
+    // kernels; a band holds at least `band_cbs` codeblocks and there are at
+    // most `max_bands` of them (bpc_set_host_pipeline)
+    static constexpr int kMaxStreams = 16;
+    int band_cbs = 512, max_bands = 32, nstreams = 16, ramp = 3;
+    cudaStream_t streams[kMaxStreams] = {};
+    cudaEvent_t done[kMaxStreams] = {};
 };
 
 DropInState &state() {
@@ -103,6 +106,42 @@ int code_device(bool enc, const int *in, int *out, int X, int Y, const int *d_lu
         }                                                                                        \
     } while (0)
 
+// Bands of codeblock rows for the host-buffer pipeline, as the row where each
+// band starts plus `rows` at the end.  The input rows and the output slots of
+// a band are contiguous in both layouts (coefficients row-major, slots in
+// raster order of codeblocks).  Bands hold at least band_cbs codeblocks (each
+// band's kernel still spreads over the SMs) and there are at most max_bands of
+// the steady length (shorter fill and drain on large images).  With ramp > 0
+// the first and the last `ramp` bands are shorter, halving towards both ends,
+// so the first kernel starts after a short copy-in and the last copy-out is
+// short too.  Bands go round-robin over the streams, so a band's copy-in waits
+// at most behind the band nstreams places earlier.
+std::vector<int> band_cuts(int rows, int ncbx, int band_cbs, int max_bands, int ramp) {
+    long long nb = (long long)rows * ncbx / band_cbs;
+    nb = nb < 1 ? 1 : (nb > max_bands ? max_bands : nb);
+    if (nb > rows) nb = rows;
+    const int len = (int)((rows + nb - 1) / nb);  // steady band length in rows
+    std::vector<int> edge;                         // ramp lengths, shortest first
+    for (int i = ramp; i >= 1; --i)
+        if ((len >> i) >= 1) edge.push_back(len >> i);
+    int e = 0;
+    for (int l : edge) e += l;
+    std::vector<int> lens;
+    if (2 * e >= rows) {
+        edge.clear();
+        e = 0;
+    }
+    lens.insert(lens.end(), edge.begin(), edge.end());
+    const int mid = rows - 2 * e;
+    const int nmid = mid > 0 ? (mid + len - 1) / len : 0;
+    for (int k = 0; k < nmid; k++) lens.push_back((int)((long long)mid * (k + 1) / nmid - (long long)mid * k / nmid));
+    lens.insert(lens.end(), edge.rbegin(), edge.rend());
+    std::vector<int> cuts{0};
+    for (int l : lens)
+        if (l > 0) cuts.push_back(cuts.back() + l);
+    return cuts;
+}
+
 // Host-buffer coding through the reusable device buffers of the drop-in state.
 int code_host_locked(DropInState &s, int direction, int *hdata, int X, int Y, const int *d_lut, int lut_n,
                      int passes, int levels, int cb) {
@@ -120,31 +159,21 @@ int code_host_locked(DropInState &s, int direction, int *hdata, int X, int Y, co
         s.cap = n;
     }
     if (!s.d_status) CUDA_TRY(cudaMalloc((void **)&s.d_status, sizeof(int)));
-    if (!s.streams[0])
-        for (int k = 0; k < DropInState::kStreams; k++) {
+    const int nst = s.nstreams;
+    for (int k = 0; k < nst; k++)
+        if (!s.streams[k]) {
             CUDA_TRY(cudaStreamCreateWithFlags(&s.streams[k], cudaStreamNonBlocking));
             CUDA_TRY(cudaEventCreateWithFlags(&s.done[k], cudaEventDisableTiming));
         }
     CUDA_TRY(cudaMemsetAsync(s.d_status, 0, sizeof(int), s.streams[0]));
     CUDA_TRY(cudaEventRecord(s.done[0], s.streams[0]));
-    for (int k = 1; k < DropInState::kStreams; k++) CUDA_TRY(cudaStreamWaitEvent(s.streams[k], s.done[0], 0));
-    // bands of codeblock rows: the input rows and the output slots of a band
-    // are contiguous in both layouts (coefficients row-major, slots in raster
-    // order of codeblocks)
+    for (int k = 1; k < nst; k++) CUDA_TRY(cudaStreamWaitEvent(s.streams[k], s.done[0], 0));
     const int ncbx = X / cb, rows = Y / cb;
-    // bands of at least 512 codeblocks (each band's kernel still spreads over
-    // the SMs), at most 32 (shorter pipeline fill and drain on large images);
-    // bands go round-robin over the 8 streams, so a band's copy-in waits at
-    // most behind the band 8 places earlier
-    const long long ncb = (long long)ncbx * rows;
-    int nband = (int)(ncb / 512);
-    nband = nband < 1 ? 1 : (nband > 32 ? 32 : nband);
-    if (nband > rows) nband = rows;
+    const std::vector<int> cuts = band_cuts(rows, ncbx, s.band_cbs, s.max_bands, s.ramp);
     const size_t row_words = (size_t)X * (size_t)cb;  // one codeblock row, either layout
-    for (int k = 0; k < nband; k++) {
-        const int r0 = (int)((long long)rows * k / nband), r1 = (int)((long long)rows * (k + 1) / nband);
-        if (r1 <= r0) continue;
-        cudaStream_t st = s.streams[k % DropInState::kStreams];
+    for (int k = 0; k + 1 < (int)cuts.size(); k++) {
+        const int r0 = cuts[k], r1 = cuts[k + 1];
+        cudaStream_t st = s.streams[k % nst];
         const size_t off = (size_t)r0 * row_words, cnt = (size_t)(r1 - r0) * row_words;
         CUDA_TRY(cudaMemcpyAsync(s.d_a + off, hdata + off, cnt * sizeof(int), cudaMemcpyHostToDevice, st));
         const int rc = code_device(direction == BPC_CODE, s.d_a, s.d_b, X, Y, d_lut, lut_n, passes, levels, cb,
@@ -152,7 +181,7 @@ int code_host_locked(DropInState &s, int direction, int *hdata, int X, int Y, co
         if (rc) return rc;
         CUDA_TRY(cudaMemcpyAsync(hdata + off, s.d_b + off, cnt * sizeof(int), cudaMemcpyDeviceToHost, st));
     }
-    for (int k = 1; k < DropInState::kStreams; k++) {
+    for (int k = 1; k < nst; k++) {
         CUDA_TRY(cudaEventRecord(s.done[k], s.streams[k]));
         CUDA_TRY(cudaStreamWaitEvent(s.streams[0], s.done[k], 0));
     }
@@ -206,6 +235,42 @@ int bpc_get_mode(int *passes, int *dwt_levels, int *cb_size) {
     if (dwt_levels) *dwt_levels = s.levels;
     if (cb_size) *cb_size = s.cb;
     return BPC_OK;
+}
+
+int bpc_set_host_pipeline(int band_cbs, int max_bands, int streams, int ramp) {
+    if (band_cbs < 1 || max_bands < 1 || max_bands > 4096 || streams < 1 || streams > DropInState::kMaxStreams ||
+        ramp < 0 || ramp > 8)
+        return BPC_ERR_ARG;
+    DropInState &s = state();
+    std::lock_guard<std::mutex> g(s.mu);
+    s.band_cbs = band_cbs;
+    s.max_bands = max_bands;
+    s.nstreams = streams;
+    s.ramp = ramp;
+    return BPC_OK;
+}
+
+int bpc_get_host_pipeline(int *band_cbs, int *max_bands, int *streams, int *ramp) {
+    DropInState &s = state();
+    std::lock_guard<std::mutex> g(s.mu);
+    if (band_cbs) *band_cbs = s.band_cbs;
+    if (max_bands) *max_bands = s.max_bands;
+    if (streams) *streams = s.nstreams;
+    if (ramp) *ramp = s.ramp;
+    return BPC_OK;
+}
+
+int bpc_host_band_rows(int X, int Y, int cb_size, int *starts, int capacity) {
+    if ((cb_size != 64 && cb_size != 32) || !valid_geometry(X, Y, cb_size, 1) || capacity < 0) return BPC_ERR_ARG;
+    DropInState &s = state();
+    std::vector<int> cuts;
+    {
+        std::lock_guard<std::mutex> g(s.mu);
+        cuts = band_cuts(Y / cb_size, X / cb_size, s.band_cbs, s.max_bands, s.ramp);
+    }
+    const int nb = (int)cuts.size() - 1;
+    for (int k = 0; starts && k < nb && k < capacity; k++) starts[k] = cuts[k];
+    return nb;
 }
 
 int bpc_last_status(void) {

@@ -90,6 +90,19 @@ int bpc_lut_free(int *d_lut);
 int bpc_code_host(int direction, int *hdata, int X, int Y, const int *d_lut, int lut_n, int passes, int levels,
                   int cb_size);
 
+/* Copy/compute pipeline of the host-buffer calls (CUDA_BPC, bpc_code_host):
+ * the image is cut into bands of codeblock rows of at least band_cbs
+ * codeblocks, at most max_bands of them at the steady length, each band's copy
+ * in, kernel and copy out queued round-robin on `streams` (1..16) CUDA
+ * streams; with ramp (0..8) > 0 the first and last `ramp` bands halve in
+ * length towards both ends of the image.  Affects the speed only; the output
+ * is the same for every setting.  bpc_host_band_rows returns the number of
+ * bands for an X x Y image and writes the first codeblock row of each (up to
+ * `capacity`) to `starts` (may be NULL). */
+int bpc_set_host_pipeline(int band_cbs, int max_bands, int streams, int ramp);
+int bpc_get_host_pipeline(int *band_cbs, int *max_bands, int *streams, int *ramp);
+int bpc_host_band_rows(int X, int Y, int cb_size, int *starts, int capacity);
+
 /* ---------------------------------------------------------------------------
  * Device-pointer entry points: stream-ordered, no allocation, no host sync.
  * ------------------------------------------------------------------------- */

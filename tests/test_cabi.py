@@ -37,6 +37,43 @@ def test_mode_validation(bpc):
     bpc.set_mode(2, 5, 64)
 
 
+def test_host_pipeline_validation(bpc):
+    before = bpc.get_host_pipeline()
+    assert before[0] >= 1 and before[1] >= 1 and 1 <= before[2] <= 16 and 0 <= before[3] <= 8
+    for bad in ((0, 32, 8, 0), (512, 0, 8, 0), (512, 32, 0, 0), (512, 32, 17, 0), (512, 32, 8, -1), (512, 32, 8, 9)):
+        assert bpc.lib().bpc_set_host_pipeline(*bad) == bpc.ERR_ARG
+    assert bpc.get_host_pipeline() == before
+    bpc.set_host_pipeline(128, 64, 16, 2)
+    assert bpc.get_host_pipeline() == (128, 64, 16, 2)
+    bpc.set_host_pipeline(*before)
+
+
+@pytest.mark.parametrize("side,cb", [(64, 64), (2048, 64), (4096, 64), (4096, 32), (16384, 64), (3072, 64), (192, 32)])
+@pytest.mark.parametrize("setting", [(512, 32, 8, 0), (256, 32, 16, 2), (128, 128, 16, 3), (64, 4096, 4, 8),
+                                     (1, 1, 1, 0), (1 << 20, 32, 8, 2)])
+def test_host_band_plan(bpc, side, cb, setting):
+    """Bands tile the codeblock rows in order; the steady length follows the
+    setting and the ramp bands halve towards both ends."""
+    before = bpc.get_host_pipeline()
+    try:
+        bpc.set_host_pipeline(*setting)
+        band_cbs, max_bands, _, ramp = setting
+        rows, ncbx = side // cb, side // cb
+        starts = bpc.host_band_rows(side, side, cb)
+        lens = [b - a for a, b in zip(starts, starts[1:] + [rows])]
+        assert starts[0] == 0 and all(l >= 1 for l in lens) and sum(lens) == rows
+        nb = min(max(rows * ncbx // band_cbs, 1), max_bands, rows)
+        steady = -(-rows // nb)
+        assert max(lens) <= steady
+        edge = [steady >> i for i in range(ramp, 0, -1) if steady >> i >= 1]
+        if edge and 2 * sum(edge) < rows:
+            assert lens[:len(edge)] == edge and lens[len(lens) - len(edge):] == edge[::-1]
+        else:
+            assert len(lens) == -(-rows // steady)
+    finally:
+        bpc.set_host_pipeline(*before)
+
+
 def test_status_strings(bpc):
     assert bpc.status_string(0) == "ok"
     assert "overflow" in bpc.status_string(bpc.ST_SLOT_OVERFLOW)
