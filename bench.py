@@ -28,8 +28,9 @@ import time
 
 import numpy as np
 
-# the request server runs small and large requests on separate streams; give
-# each stream its own hardware queue (must be set before CUDA initialises)
+# the request server runs small and large requests on separate streams and the
+# host-buffer path pipelines bands on 16 streams; give each stream its own
+# hardware queue (must be set before CUDA initialises)
 os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
 ROOT = os.path.dirname(os.path.abspath(__file__))
 PKG = os.path.join(ROOT, "cuda_bpc-paco_b200")

@@ -131,6 +131,34 @@ def test_device_api_and_persistent_grid(bpc, oracle_mod):
         lut.close()
 
 
+@pytest.mark.parametrize("cb", [64, 32])
+def test_host_pipeline_settings(bpc, cb):
+    """The host-buffer path gives the device path's stream and a lossless
+    decode for every band plan: one band on one stream, many one-row bands,
+    ramped bands, more bands than streams."""
+    import torch
+    img = synth(2048, 5, 21, amp=30, nrect=20)
+    lut = bpc.DeviceLut(lut_folder(3), 3, 5)
+    before = bpc.get_host_pipeline()
+    try:
+        d = torch.from_numpy(img).cuda()
+        want = torch.empty_like(d)
+        st = torch.zeros(1, dtype=torch.int32, device="cuda")
+        bpc.encode_device(d, want, lut, cb, st)
+        want = want.cpu().numpy().reshape(-1)
+        for setting in ((1, 1, 1, 0), (1, 4096, 16, 0), (512, 32, 16, 3), (128, 7, 3, 1), (64, 4096, 2, 8)):
+            bpc.set_host_pipeline(*setting)
+            got, est = bpc.encode_host(img, lut, cb)
+            assert est == 0
+            np.testing.assert_array_equal(got, want, err_msg=str(setting))
+            dec, dst = bpc.decode_host(got, img.shape, lut, cb)
+            assert dst == 0
+            np.testing.assert_array_equal(dec, img, err_msg=str(setting))
+    finally:
+        bpc.set_host_pipeline(*before)
+        lut.close()
+
+
 def test_drop_in_flow(bpc, oracle_mod, sample_subset):
     """main_example.cu:498-532: load_LUTs, CUDA_BPC(CODE), load_LUTs again
     (CUDA_BPC frees it), CUDA_BPC(DECODE), compare."""
