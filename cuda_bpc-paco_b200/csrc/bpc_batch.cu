@@ -105,8 +105,8 @@ __global__ void __launch_bounds__(kWarps * 32, ENC ? kMinCtasEnc : kMinCtasDec)
     uint32_t *ring = reinterpret_cast<uint32_t *>(smem + kSignTableBytes) + warp * (ENC ? 512 : G::RING_WORDS);
     GpuWarpB w;
     uint32_t planes[28][4];
-    uint8_t ev_key[ENC ? 256 : 1];
-    uint32_t ev_val[ENC ? 256 : 1];
+    uint8_t ev_key[ENC ? kEvKeys : 1];
+    uint32_t ev_val[ENC ? kEvVals : 1];
     for (;;) {
         unsigned it = 0;
         if (w.lane() == 0) it = atomicAdd(head, 1u);

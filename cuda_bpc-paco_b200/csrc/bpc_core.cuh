@@ -244,14 +244,21 @@ struct Lane {
     uint32_t lower, size, resv, cw;
     uint32_t cnt;      // codewords reserved in this codeblock (group-uniform)
     uint32_t ring_hi;  // decoder: slot words [ring_hi - RING, ring_hi) are in the ring
-    int has_resv;
     int status;
-    // encoder: slot of the open codeword (-1: reserved in the current chunk,
-    // slot not ranked yet) and the chunk's event list length
+    // encoder: slot of the codeword left open by an earlier pass (-1: none),
+    // the ev_val index the open codeword finishes into (its event in this
+    // pass, or kEvOpen) and the pass's event count
     int open_slot;
     int cur_ev;
     int nev;
 };
+
+// Sizes of the encoder's per-lane event arrays.  ev_key holds one pass's
+// reservations: at most one per symbol call, and a lane makes at most two
+// calls per coefficient of its stripe (256 for 64x64, 128 for 32x32).  ev_val
+// has one more word, the value of a codeword reserved in an earlier pass
+// (kEvOpen).
+constexpr int kEvKeys = 256, kEvOpen = 256, kEvVals = 257;
 
 // Decoder codeword ring refill: lane gl of a codeblock's lane group copies
 // its share of slot words [first, first + nwords) into the ring with 16-byte
@@ -579,38 +586,41 @@ struct Coder {
     // warp ranks all events by (key, lane) -- the reference's lockstep order --
     // and the codewords go to their slots.
 
-    // Arithmetic_encoder :261-295 for this lane; reservation -> event.  `on`
-    // predicates the call so that the optional sign call needs no branch.
+    // Arithmetic_encoder :261-295 for this lane, with predicated stores
+    // instead of branches (lanes reserve and finish codewords at different
+    // symbols, and a branch per case would serialise the warp).  A reservation
+    // (:268-279) appends an event (its key; the slot is ranked at the end of
+    // the pass); a finished codeword (Size == 0) stores its value with its
+    // event, or in ev_val[kEvOpen] if it was reserved in an earlier pass.
+    // `on` predicates the call (the optional sign call).
     BPC_FI void enc_symbol_if(bool on, uint32_t sym, uint32_t P, int key) {
-        if (on && s.size == 0) {
-            ev_key[s.nev] = (uint8_t)key;  // its value is stored when the codeword completes
-            s.cur_ev = s.nev;
-            s.nev++;
-            w.smem_or(&evmask[key], 1u << lane);
-            s.has_resv = 1;
-            s.lower = 0;
-            s.size = 0xFFFFu;
-        }
-        const uint32_t t = ((s.size * P) >> 7) + sym;
-        const uint32_t nsize = sym ? s.size - t : t;
-        const uint32_t nlow = sym ? s.lower + t : s.lower;
-        if (on) {
-            s.size = nsize;
-            s.lower = nlow;
-        }
-        if (on && nsize == 0) {
-            if (s.cur_ev >= 0)
-                ev_val[s.cur_ev] = nlow;
-            else if (s.open_slot < G::CAP)
-                slot_out[s.open_slot] = (int32_t)nlow;
-            else
-                s.status |= ST_OVERFLOW;
-        }
+        const bool rs = on && s.size == 0;
+        if (rs) ev_key[s.nev] = (uint8_t)key;
+        s.cur_ev = rs ? s.nev : s.cur_ev;
+        s.nev += rs ? 1 : 0;
+        const uint32_t size0 = rs ? 0xFFFFu : s.size, low0 = rs ? 0u : s.lower;
+        const uint32_t t = ((size0 * P) >> 7) + sym;
+        const uint32_t nsize = sym ? size0 - t : t;
+        const uint32_t nlow = sym ? low0 + t : low0;
+        const bool fin = on && nsize == 0;
+        if (fin) ev_val[s.cur_ev] = nlow;
+        s.size = on ? nsize : s.size;
+        s.lower = on ? nlow : s.lower;
     }
 
     // Rank the pass's events by (key, lane) and store completed codewords.
     BPC_FI void enc_rank() {
+        // The codeword left open by an earlier pass finished in this one if the
+        // lane reserved again (a reservation needs Size == 0) or ends at Size 0.
+        if (s.open_slot >= 0 && (s.nev > 0 || s.size == 0)) {
+            if ((uint32_t)s.open_slot < (uint32_t)G::CAP)
+                slot_out[s.open_slot] = (int32_t)ev_val[kEvOpen];
+            else
+                s.status |= ST_OVERFLOW;
+            s.open_slot = -1;
+        }
         if (!w.any(s.nev > 0)) return;
+        for (int e = 0; e < s.nev; e++) w.smem_or(&evmask[ev_key[e]], 1u << lane);
         w.sync();
         uint32_t c[8], v = 0;
 #pragma unroll
@@ -649,7 +659,7 @@ struct Coder {
             }
         }
         s.cnt += (tot >> sh) & hm;
-        s.cur_ev = -1;
+        s.cur_ev = kEvOpen;  // a codeword still open finishes into ev_val[kEvOpen]
         s.nev = 0;
         w.sync();
 #pragma unroll
@@ -977,10 +987,9 @@ struct Coder {
         s.XL = s.XR = s.XNL = s.XNR = 0ull;
         s.lower = s.size = s.resv = s.cw = 0u;
         s.cnt = 0u;
-        s.has_resv = 0;
         s.status = 0;
         s.open_slot = -1;
-        s.cur_ev = -1;
+        s.cur_ev = kEvOpen;
         s.nev = 0;
         XLS = XRS = XLN = XRN = 0ull;
         if (ENC) {
@@ -1095,8 +1104,8 @@ struct Coder {
         }
         if (ENC) {
             if (ok && !STATS) {
-                if (s.has_resv && s.size != 0) {  // flush :1020 (a finished codeword is already stored)
-                    if (s.open_slot < G::CAP)
+                if (s.size != 0) {  // flush :1020 (a finished codeword is already stored)
+                    if ((uint32_t)s.open_slot < (uint32_t)G::CAP)
                         slot_out[s.open_slot] = (int32_t)s.lower;
                     else
                         s.status |= ST_OVERFLOW;

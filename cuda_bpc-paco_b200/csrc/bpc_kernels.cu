@@ -70,8 +70,8 @@ __global__ void __launch_bounds__(kWarps * 32, ENC ? kMinCtasEnc : kMinCtasDec) 
         reinterpret_cast<uint32_t *>(smem + p.tab_n + kSignTableBytes) + warp * (ENC ? 512 : G::RING_WORDS);
     GpuWarp w;
     uint32_t planes[28][4];  // per-thread bitplanes (local memory, L1-resident)
-    uint8_t ev_key[ENC ? 256 : 1];
-    uint32_t ev_val[ENC ? 256 : 1];
+    uint8_t ev_key[ENC ? kEvKeys : 1];
+    uint32_t ev_val[ENC ? kEvVals : 1];
     const int stride = (int)gridDim.x * kWarps * G::NG;
     for (int base = p.cb_begin + ((int)blockIdx.x * kWarps + warp) * G::NG; base < p.cb_end; base += stride) {
         Coder<PASSES, CBS, ENC, GpuWarp> cd(w, p, ring, tab, sgtab, planes, ev_key, ev_val);

@@ -118,8 +118,8 @@ void lane_main() {
     const int l = S->cur;
     EmuWarp w{l};
     uint32_t planes[28][4];
-    uint8_t ev_key[ENC ? 256 : 1];
-    uint32_t ev_val[ENC ? 256 : 1];
+    uint8_t ev_key[ENC ? bpc::kEvKeys : 1];
+    uint32_t ev_val[ENC ? bpc::kEvVals : 1];
     bpc::Coder<PASSES, CBS, ENC, EmuWarp> cd(w, *J->p, J->ring, J->tab, J->sgtab, planes, ev_key, ev_val);
     if constexpr (ENC) {
         if (J->kind == 1)
