@@ -58,6 +58,16 @@ def workload_name(c):
     return f"{c['side']}x{c['side']} {src}, {c['cb']}x{c['cb']} codeblocks, {c['passes']}-pass encode+decode"
 
 
+def launches_per_call(X, Y, cb, enc, dev):
+    """Kernels one work-ordered call launches: the coder, plus the cost and
+    sort kernels when the image spans more than two waves of resident warps
+    (4 warps x 4 encoder / 7 decoder CTAs per SM)."""
+    import torch
+    units = (X // cb) * (Y // cb) // (1 if cb == 64 else 2)
+    resident = torch.cuda.get_device_properties(dev).multi_processor_count * 4 * (4 if enc else 7)
+    return 3 if units >= 2 * resident else 1
+
+
 def load_peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -542,16 +552,19 @@ def run_ours(args, c):
     d_dec = torch.empty_like(d_img)
     d_status = torch.zeros(1, dtype=torch.int32, device=dev)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    # work-ordered calls: images of more than two warp waves are coded heaviest
+    # codeblocks first (two small planning kernels inside the timed call)
+    sched = bpc.sched_buffer(X, Y, cb)
 
     def step(times=None):
         flush.fill_(1)
         e0, e1, e2, e3 = (torch.cuda.Event(enable_timing=True) for _ in range(4))
         e0.record(stream)
-        bpc.encode_device(d_img, d_stream, lut, cb, d_status)
+        bpc.encode_device(d_img, d_stream, lut, cb, d_status, sched=sched)
         e1.record(stream)
         flush.fill_(2)
         e2.record(stream)
-        bpc.decode_device(d_stream, d_dec, lut, cb, d_status)
+        bpc.decode_device(d_stream, d_dec, lut, cb, d_status, sched=sched)
         e3.record(stream)
         if times is not None:
             times.append((e0, e1, e2, e3))
@@ -629,7 +642,7 @@ def run_ours(args, c):
                    "l2": "flushed (256 MiB write) before every kernel", "parallelism": f"replicas x{world}"},
         "encode_gcoeffs": N / te1 / 1e9, "decode_gcoeffs": N / td1 / 1e9,
         "e2e": {"value": e2e, "unit": "Gcoeff/s", "h2d_bytes_per_step": 2 * 4 * N, "d2h_bytes_per_step": 2 * 4 * N + 8},
-        "gpu_launches": 2 * args.steps,
+        "gpu_launches": args.steps * (launches_per_call(X, Y, cb, True, dev) + launches_per_call(X, Y, cb, False, dev)),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": NCU_TRAFFIC.get(args.config), "peak_source": peak_kind,
                      "kernel": "k_bpc decoder" if td1 >= te1 else "k_bpc encoder",

@@ -58,6 +58,14 @@ def lib() -> ctypes.CDLL:
                ctypes.c_int, vp]
         L.bpc_encode_device.argtypes = dev
         L.bpc_decode_device.argtypes = dev
+        L.bpc_sched_ints.argtypes = [ctypes.c_int] * 3
+        L.bpc_sched_ints.restype = ctypes.c_longlong
+        dev_s = [vp, vp, ctypes.c_int, ctypes.c_int, vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp, vp,
+                 vp, vp]
+        L.bpc_encode_device_sched.argtypes = dev_s
+        L.bpc_decode_device_sched.argtypes = dev_s
+        L.bpc_encode_device_sched.restype = ctypes.c_int
+        L.bpc_decode_device_sched.restype = ctypes.c_int
         L.bpc_lut_entries.argtypes = [ctypes.c_int] * 3
         L.bpc_set_host_pipeline.argtypes = [ctypes.c_int] * 4
         L.bpc_get_host_pipeline.argtypes = [ip, ip, ip, ip]
@@ -182,23 +190,43 @@ def _ptr(t) -> int:
     return 0 if t is None else int(t.data_ptr())
 
 
+def sched_buffer(X: int, Y: int, cb: int = 64):
+    """Device scratch for the work-ordered calls (bpc_sched_ints ints)."""
+    import torch
+    n = _check(lib().bpc_sched_ints(X, Y, cb), "bpc_sched_ints")
+    return torch.empty(max(n, 1), dtype=torch.int32, device="cuda")
+
+
 def encode_device(coeffs, stream_out, lut: DeviceLut, cb: int = 64, status=None, counts=None, grid: int = 0,
-                  cuda_stream: int | None = None) -> None:
+                  cuda_stream: int | None = None, sched=None) -> None:
     """Device-to-device encode of torch int32 tensors (Y x X coeffs -> X*Y
-    stream), enqueued on `cuda_stream` (default: torch's current stream)."""
+    stream), enqueued on `cuda_stream` (default: torch's current stream).
+    With `sched` (sched_buffer) large images are coded in work order."""
     import torch
     Y, X = coeffs.shape
     s = torch.cuda.current_stream().cuda_stream if cuda_stream is None else cuda_stream
+    if sched is not None:
+        _check(lib().bpc_encode_device_sched(_ptr(coeffs), _ptr(stream_out), X, Y, ctypes.c_void_p(lut.ptr), lut.n,
+                                             lut.passes, lut.levels, cb, ctypes.c_void_p(_ptr(status)),
+                                             ctypes.c_void_p(_ptr(counts)), ctypes.c_void_p(_ptr(sched)),
+                                             ctypes.c_void_p(s)), "bpc_encode_device_sched")
+        return
     _check(lib().bpc_encode_device(_ptr(coeffs), _ptr(stream_out), X, Y, ctypes.c_void_p(lut.ptr), lut.n, lut.passes,
                                    lut.levels, cb, ctypes.c_void_p(_ptr(status)), ctypes.c_void_p(_ptr(counts)), grid,
                                    ctypes.c_void_p(s)), "bpc_encode_device")
 
 
 def decode_device(stream_in, coeffs_out, lut: DeviceLut, cb: int = 64, status=None, counts=None, grid: int = 0,
-                  cuda_stream: int | None = None) -> None:
+                  cuda_stream: int | None = None, sched=None) -> None:
     import torch
     Y, X = coeffs_out.shape
     s = torch.cuda.current_stream().cuda_stream if cuda_stream is None else cuda_stream
+    if sched is not None:
+        _check(lib().bpc_decode_device_sched(_ptr(stream_in), _ptr(coeffs_out), X, Y, ctypes.c_void_p(lut.ptr),
+                                             lut.n, lut.passes, lut.levels, cb, ctypes.c_void_p(_ptr(status)),
+                                             ctypes.c_void_p(_ptr(counts)), ctypes.c_void_p(_ptr(sched)),
+                                             ctypes.c_void_p(s)), "bpc_decode_device_sched")
+        return
     _check(lib().bpc_decode_device(_ptr(stream_in), _ptr(coeffs_out), X, Y, ctypes.c_void_p(lut.ptr), lut.n,
                                    lut.passes, lut.levels, cb, ctypes.c_void_p(_ptr(status)),
                                    ctypes.c_void_p(_ptr(counts)), grid, ctypes.c_void_p(s)), "bpc_decode_device")

@@ -16,7 +16,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libbpc_paco.so")
-SOURCES = ["bpc_kernels.cu", "bpc_api.cu", "bpc_batch.cu", "bpc_noalloc.cu", "bpc_dwt.cu", "bpc_server.cu",
+SOURCES = ["bpc_kernels.cu", "bpc_order.cu", "bpc_api.cu", "bpc_batch.cu", "bpc_noalloc.cu", "bpc_dwt.cu", "bpc_server.cu",
            "bpc_train.cu", "bpc_lut.cpp", "bpc_files.cpp"]
 HEADERS = ["bpc_core.cuh", "bpc_kernels.h", "bpc_lut.h", "bpc_arena.h"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")

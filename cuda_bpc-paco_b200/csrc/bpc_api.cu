@@ -81,13 +81,21 @@ int fill_params(bpc::Params &p, const int *in, int *out, int X, int Y, const int
 }
 
 int code_device(bool enc, const int *in, int *out, int X, int Y, const int *d_lut, int lut_n, int passes, int levels,
-                int cb, int *d_status, int *d_counts, int grid, void *stream, int cb_begin = 0, int cb_end = -1) {
+                int cb, int *d_status, int *d_counts, int grid, void *stream, int cb_begin = 0, int cb_end = -1,
+                int *sched = nullptr) {
     bpc::Params p;
     const int rc = fill_params(p, in, out, X, Y, d_lut, lut_n, passes, levels, cb, d_status, d_counts);
     if (rc) return rc;
     if (cb_end >= 0) {
         p.cb_begin = cb_begin;
         p.cb_end = cb_end;
+    }
+    if (sched && grid <= 0) {
+        const cudaError_t e = bpc::plan_order(enc, cb, p, sched, (cudaStream_t)stream, &p.order);
+        if (e != cudaSuccess) {
+            std::fprintf(stderr, "bpc: work-order launch failed: %s\n", cudaGetErrorString(e));
+            return BPC_ERR_CUDA;
+        }
     }
     const cudaError_t e = bpc::launch_code(enc, passes, cb, p, grid, (cudaStream_t)stream);
     if (e != cudaSuccess) {
@@ -345,6 +353,25 @@ int bpc_decode_device(const int *d_stream, int *d_coeffs, int X, int Y, const in
                       int levels, int cb_size, int *d_status, int *d_counts, int grid, void *stream) {
     return code_device(false, d_stream, d_coeffs, X, Y, d_lut, lut_n, passes, levels, cb_size, d_status, d_counts,
                        grid, stream);
+}
+
+long long bpc_sched_ints(int X, int Y, int cb_size) {
+    if ((cb_size != 64 && cb_size != 32) || !valid_geometry(X, Y, cb_size, 1)) return BPC_ERR_ARG;
+    return bpc::sched_ints((X / cb_size) * (Y / cb_size), cb_size);
+}
+
+int bpc_encode_device_sched(const int *d_coeffs, int *d_stream, int X, int Y, const int *d_lut, int lut_n, int passes,
+                            int levels, int cb_size, int *d_status, int *d_counts, int *d_sched, void *stream) {
+    if (!d_sched) return BPC_ERR_ARG;
+    return code_device(true, d_coeffs, d_stream, X, Y, d_lut, lut_n, passes, levels, cb_size, d_status, d_counts, 0,
+                       stream, 0, -1, d_sched);
+}
+
+int bpc_decode_device_sched(const int *d_stream, int *d_coeffs, int X, int Y, const int *d_lut, int lut_n, int passes,
+                            int levels, int cb_size, int *d_status, int *d_counts, int *d_sched, void *stream) {
+    if (!d_sched) return BPC_ERR_ARG;
+    return code_device(false, d_stream, d_coeffs, X, Y, d_lut, lut_n, passes, levels, cb_size, d_status, d_counts, 0,
+                       stream, 0, -1, d_sched);
 }
 
 void load_LUTs(int **LUT, const char *folder) {

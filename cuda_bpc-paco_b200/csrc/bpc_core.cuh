@@ -83,6 +83,9 @@ struct Params {
     // codewords) are in[offsets[k] .. offsets[k+1]); null = slot layout
     const long long *offsets;
     int cb_begin, cb_end;  // codeblocks [cb_begin, cb_end) of the image are coded by this launch
+    // work order of a whole-image launch: warp slot k codes the codeblocks
+    // starting at order[k] (null = raster order)
+    const int *order = nullptr;
 };
 
 // LUT offsets the reference kernel uses (Initialize_LUT_pointers :228-250 with

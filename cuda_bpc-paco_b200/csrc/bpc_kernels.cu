@@ -75,7 +75,7 @@ __global__ void __launch_bounds__(kWarps * 32, ENC ? kMinCtasEnc : kMinCtasDec) 
     const int stride = (int)gridDim.x * kWarps * G::NG;
     for (int base = p.cb_begin + ((int)blockIdx.x * kWarps + warp) * G::NG; base < p.cb_end; base += stride) {
         Coder<PASSES, CBS, ENC, GpuWarp> cd(w, p, ring, tab, sgtab, planes, ev_key, ev_val);
-        cd.run(base);
+        cd.run(p.order ? p.order[base / G::NG] : base);
     }
 }
 

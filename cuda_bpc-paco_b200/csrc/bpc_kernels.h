@@ -27,6 +27,14 @@ constexpr int kMinCtasEnc = ENC_MIN_CTAS;
 // walk the codeblocks grid-stride.
 cudaError_t launch_code(bool enc, int passes, int cbs, const Params &p, int grid, cudaStream_t st);
 
+// Work order for a whole-image launch of many warp waves (bpc_order.cu): with
+// scratch `sched` of sched_ints(ncb, cbs) ints, queue the kernels that sort
+// the image's work units by expected cost and set *order to the order to put
+// in Params; *order stays null (raster order) for images of at most two waves.
+long long sched_ints(int ncb, int cbs);
+bool order_pays(bool enc, int ncb, int cbs);  // more than two waves on this device
+cudaError_t plan_order(bool enc, int cbs, const Params &p, int *sched, cudaStream_t st, const int **order);
+
 // LUT training: add, per LUT entry, [2k] symbols coded and [2k+1] symbols
 // equal to 1 over p.ncb codeblocks of p.in (planes 0..14) to stats.
 cudaError_t launch_stats(int passes, int cbs, const Params &p, unsigned long long *stats, cudaStream_t st);

@@ -11,8 +11,9 @@
 // Scheduling.  Requests are admitted strictly in arrival order (no request can
 // starve behind smaller ones) whenever one of the `max_in_flight` streams is
 // free and the head request's output fits in the arena.  Each admitted request
-// is one launch of the plain coder on its own stream, followed by a 4-byte
-// copy of its status word and an event; launches on different streams run
+// is one launch of the plain coder (work-ordered for requests of more than two
+// warp waves, its scratch allocated with the output) on its own stream,
+// followed by a 4-byte copy of its status word and an event; launches on different streams run
 // concurrently, so the CTAs of a newly admitted request fill the SMs that an
 // earlier request's tail leaves idle.  Each slot has one stream per priority
 // class (up to three hardware priority levels) and a request runs in the class
@@ -41,6 +42,7 @@
 
 #include "../../include/bpc_paco.h"
 #include "bpc_arena.h"
+#include "bpc_kernels.h"
 
 namespace {
 
@@ -56,7 +58,8 @@ struct Request {
     int dir;
     const int *in;
     int X, Y, lut, cb;
-    size_t bytes;
+    size_t bytes;        // output, plus the work-order scratch when sched_off > 0
+    size_t sched_off;    // byte offset of that scratch in the allocation (0: none)
     Clock::time_point t0;
 };
 
@@ -124,7 +127,13 @@ void launch(Server *s, Slot &sl) {
     int *out = reinterpret_cast<int *>(s->base + sl.off);
     sl.st = sl.st_by_prio[priority_level(r.X, r.Y, (int)sl.st_by_prio.size())];
     int rc = cudaMemsetAsync(sl.d_status, 0, sizeof(int), sl.st) == cudaSuccess ? BPC_OK : BPC_ERR_CUDA;
-    if (!rc)
+    int *sched = r.sched_off ? reinterpret_cast<int *>(s->base + sl.off + r.sched_off) : nullptr;
+    if (!rc && sched)
+        rc = r.dir == BPC_CODE ? bpc_encode_device_sched(r.in, out, r.X, r.Y, L.d, L.n, L.passes, L.levels, r.cb,
+                                                         sl.d_status, nullptr, sched, sl.st)
+                               : bpc_decode_device_sched(r.in, out, r.X, r.Y, L.d, L.n, L.passes, L.levels, r.cb,
+                                                         sl.d_status, nullptr, sched, sl.st);
+    else if (!rc)
         rc = r.dir == BPC_CODE ? bpc_encode_device(r.in, out, r.X, r.Y, L.d, L.n, L.passes, L.levels, r.cb,
                                                    sl.d_status, nullptr, 0, sl.st)
                                : bpc_decode_device(r.in, out, r.X, r.Y, L.d, L.n, L.passes, L.levels, r.cb,
@@ -259,12 +268,18 @@ extern "C" long long bpc_server_submit(void *srv, int direction, const int *d_in
     if (!s || !d_in || (direction != BPC_CODE && direction != BPC_DECODE) || (cb_size != 64 && cb_size != 32) ||
         X <= 0 || Y <= 0 || X % cb_size || Y % cb_size)
         return BPC_ERR_ARG;
-    const size_t bytes = ((size_t)X * (size_t)Y * sizeof(int) + kAlign - 1) / kAlign * kAlign;
+    size_t bytes = ((size_t)X * (size_t)Y * sizeof(int) + kAlign - 1) / kAlign * kAlign;
+    size_t sched_off = 0;
+    const int ncb = (X / cb_size) * (Y / cb_size);
+    if (bpc::order_pays(direction == BPC_CODE, ncb, cb_size)) {  // large request: work-ordered coding
+        sched_off = bytes;
+        bytes += ((size_t)bpc::sched_ints(ncb, cb_size) * sizeof(int) + kAlign - 1) / kAlign * kAlign;
+    }
     std::lock_guard<std::mutex> g(s->mu);
     if (lut_id < 0 || lut_id >= (int)s->luts.size() || s->stop) return BPC_ERR_ARG;
     if (bytes > s->budget) return BPC_ERR_TOO_LARGE;  // could never be admitted
     const long long t = s->next_ticket++;
-    s->queue.push_back({t, direction, d_in, X, Y, lut_id, cb_size, bytes, Clock::now()});
+    s->queue.push_back({t, direction, d_in, X, Y, lut_id, cb_size, bytes, sched_off, Clock::now()});
     s->cv.notify_one();
     return t;
 }

@@ -120,6 +120,21 @@ int bpc_encode_device(const int *d_coeffs, int *d_stream, int X, int Y, const in
 int bpc_decode_device(const int *d_stream, int *d_coeffs, int X, int Y, const int *d_lut, int lut_n, int passes,
                       int levels, int cb_size, int *d_status, int *d_counts, int grid, void *stream);
 
+/* The same calls with a work order: for images of more than two waves of
+ * warps (above about 4,700 codeblocks for the encoder, 8,300 for the decoder
+ * on a 148-SM B200) the call first sorts the codeblocks by expected work,
+ * heaviest first (decoder: slot words in use; encoder: bitplanes coded, from
+ * one read of the coefficients), so that the warps of a CTA finish together
+ * and the last wave is short.  Outputs are identical to the calls above.
+ * d_sched is the caller's device scratch of bpc_sched_ints(X, Y, cb_size)
+ * ints (8 bytes per 64x64 codeblock), reusable once the call's stream has
+ * passed it; still no allocation and no host sync. */
+long long bpc_sched_ints(int X, int Y, int cb_size);
+int bpc_encode_device_sched(const int *d_coeffs, int *d_stream, int X, int Y, const int *d_lut, int lut_n, int passes,
+                            int levels, int cb_size, int *d_status, int *d_counts, int *d_sched, void *stream);
+int bpc_decode_device_sched(const int *d_stream, int *d_coeffs, int X, int Y, const int *d_lut, int lut_n, int passes,
+                            int levels, int cb_size, int *d_status, int *d_counts, int *d_sched, void *stream);
+
 /* ---------------------------------------------------------------------------
  * Batched persistent coding (no counterpart in the reference, which codes one
  * image per call): many images of mixed size, DWT levels, pass count and

@@ -74,6 +74,15 @@ def test_host_band_plan(bpc, side, cb, setting):
         bpc.set_host_pipeline(*before)
 
 
+def test_sched_ints(bpc):
+    L = bpc.lib()
+    assert L.bpc_sched_ints(4096, 4096, 64) == 2 * 4096
+    assert L.bpc_sched_ints(4096, 4096, 32) == 2 * 8192
+    assert L.bpc_sched_ints(96, 64, 32) == 2 * 3  # 6 codeblocks, 3 warp units
+    for bad in ((100, 64, 64), (64, 64, 48), (0, 64, 64)):
+        assert L.bpc_sched_ints(*bad) == bpc.ERR_ARG
+
+
 def test_status_strings(bpc):
     assert bpc.status_string(0) == "ok"
     assert "overflow" in bpc.status_string(bpc.ST_SLOT_OVERFLOW)

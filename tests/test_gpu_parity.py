@@ -159,6 +159,37 @@ def test_host_pipeline_settings(bpc, cb):
         lut.close()
 
 
+@pytest.mark.parametrize("side,levels,passes,cb", [(8192, 5, 3, 64), (6144, 6, 2, 64), (6144, 5, 3, 32),
+                                                     (2048, 5, 3, 64)])
+def test_work_ordered_calls(bpc, side, levels, passes, cb):
+    """The work-ordered entry points write the same stream and coefficients as
+    the raster-order ones: images of many warp waves (sorted, 64x64 and 32x32
+    with codeblocks straddling subbands) and one within two waves (unsorted).
+    Outputs start from a sentinel, so a codeblock the order skipped shows."""
+    import torch
+    lut = bpc.DeviceLut(lut_folder(passes), passes, levels)
+    try:
+        d = bpc_synth.synthetic_coefficients_gpu(side, levels, 31, amp=60.0, nrect=100)
+        st = torch.zeros(4, dtype=torch.int32, device="cuda")  # plain enc, ordered enc, plain dec, ordered dec
+        want = torch.empty_like(d)
+        bpc.encode_device(d, want, lut, cb, st[0:1])
+        sched = bpc.sched_buffer(side, side, cb)
+        got = torch.full_like(d, 0x7F7F7F7F)
+        bpc.encode_device(d, got, lut, cb, st[1:2], sched=sched)
+        assert torch.equal(got, want)
+        want_dec = torch.empty_like(d)
+        bpc.decode_device(want, want_dec, lut, cb, st[2:3])
+        dec = torch.full_like(d, 0x7F7F7F7F)
+        bpc.decode_device(got, dec, lut, cb, st[3:4], sched=sched)
+        assert torch.equal(dec, want_dec)
+        s = st.cpu().tolist()
+        assert s[0] == s[1] and s[2] == s[3] and s[0] & ~bpc.ST_SLOT_OVERFLOW == 0
+        if s[0] == 0:
+            assert torch.equal(dec, d)
+    finally:
+        lut.close()
+
+
 def test_drop_in_flow(bpc, oracle_mod, sample_subset):
     """main_example.cu:498-532: load_LUTs, CUDA_BPC(CODE), load_LUTs again
     (CUDA_BPC frees it), CUDA_BPC(DECODE), compare."""
