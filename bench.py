@@ -49,7 +49,7 @@ CONFIGS = {
 METRIC = "encode/decode Gcoeff/s (bit-exact)"
 # DRAM read + write bytes of one launch of the dominant kernel (the decoder),
 # from the ncu capture summarised in profiles/k_bpc_cfg2_full.md.
-NCU_TRAFFIC = {"cfg2": 15.084288e6 + 18.242304e6}
+NCU_TRAFFIC = {"cfg2": 15.08992e6 + 18.553856e6}
 
 
 def workload_name(c):
