@@ -13,7 +13,7 @@
 //   decoder: the slot words in use (MSB word + codewords), found by a binary
 //            search for the first -1 of the fill (codewords are 0..0xFFFF;
 //            on a damaged slot the search still ends inside it, and only the
-//            order is affected);
+//            order is affected), plus kPlaneWords per bitplane decoded;
 //   encoder: the bitplanes coded, MSB + 1 (33 for an all-zero codeblock),
 //            from one read of the coefficients.
 // One CTA then counting-sorts the units by cost, descending (warp-aggregated
@@ -28,6 +28,10 @@ namespace bpc {
 namespace {
 
 constexpr int kBuckets = 1024;  // = threads of the sorting CTA
+// decoder cost per plane in codeword-equivalents: a lockstep pass over a plane
+// costs about as much as decoding 128 codewords (fit of per-codeblock decoder
+// cycles on a B200 to words + planes)
+constexpr uint32_t kPlaneWords = 128;
 
 template <int CBS>
 __global__ void k_cost_dec(const int32_t *in, int ncb, uint32_t *key) {
@@ -47,7 +51,9 @@ __global__ void k_cost_dec(const int32_t *in, int ncb, uint32_t *key) {
                 else
                     lo = mid + 1;
             }
-            cost += (uint32_t)lo;
+            const int m = __ldg(slot);  // MSB word: planes decoded
+            const uint32_t planes = m == 32 ? 33u : (m >= 0 && m <= 27 ? (uint32_t)m + 1u : 0u);
+            cost += (uint32_t)lo + kPlaneWords * planes;
         }
         key[u] = cost;
     }
@@ -151,8 +157,8 @@ cudaError_t plan_t(bool enc, const Params &p, int *sched, cudaStream_t st, const
         const int grid = (units + 255) / 256 < 1024 ? (units + 255) / 256 : 1024;
         k_cost_dec<CBS><<<grid, 256, 0, st>>>(p.in, p.ncb, key);
     }
-    // decoder costs reach NG * CAP words: 4096 (64x64) or 2048 (32x32)
-    const int shift = enc ? 0 : 2;
+    // decoder costs reach NG * (CAP + 33 * kPlaneWords): 8320 (64x64), 12544 (32x32)
+    const int shift = enc ? 0 : (CBS == 64 ? 3 : 4);
     k_order<<<1, kBuckets, 0, st>>>(key, units, shift, G::NG, sched);
     *order = sched;
     return cudaGetLastError();
