@@ -90,6 +90,33 @@ def test_mixed_requests_match_alone(bpc, oracle_mod, luts):
         srv.close()
 
 
+def test_large_requests_work_ordered(bpc, luts):
+    """Requests of more than two warp waves run the work-ordered coder with its
+    scratch beside the output in the arena: same words as the one-request
+    raster-order calls, and the arena is empty again after release."""
+    import torch
+    d = bpc_synth.synthetic_coefficients_gpu(8192, 5, 17, amp=60.0, nrect=100)
+    want, st = alone(bpc, torch, bpc.CODE, d, luts[3], 64)
+    srv = bpc.Server(2 * d.numel() * 4 + (8 << 20), 2)
+    try:
+        lid = srv.register_lut(luts[3])
+        t_enc = srv.submit(bpc.CODE, d.view(-1), lid, 64, shape=d.shape)
+        t_dec = srv.submit(bpc.DECODE, want.view(-1), lid, 64, shape=d.shape)
+        got = collect(srv, 2)
+        ptr, _, s_enc = got[t_enc]
+        assert s_enc == st
+        assert torch.equal(bpc.as_tensor(ptr, d.numel()), want.view(-1))
+        srv.release(ptr)
+        ptr, _, s_dec = got[t_dec]
+        dec_alone, s_alone = alone(bpc, torch, bpc.DECODE, want, luts[3], 64)
+        assert s_dec == s_alone
+        assert torch.equal(bpc.as_tensor(ptr, d.numel()), dec_alone.view(-1))
+        srv.release(ptr)
+        assert srv.state()["bytes_used"] == 0
+    finally:
+        srv.close()
+
+
 def test_budget_admission_in_order(bpc, luts):
     import torch
     img = bpc_synth.synthetic_coefficients(1024, 5, 7, amp=30, nrect=10)
