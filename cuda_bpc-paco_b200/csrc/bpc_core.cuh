@@ -154,11 +154,11 @@ BPC_FI void add_u64(unsigned long long *p, unsigned long long v) {
     *p += v;
 #endif
 }
-BPC_FI int ctz64(uint64_t x) {
+BPC_FI int ctz32(uint32_t x) {
 #if defined(__CUDA_ARCH__)
-    return __ffsll((long long)x) - 1;
+    return __ffs((int)x) - 1;
 #else
-    return __builtin_ctzll(x);
+    return __builtin_ctz(x);
 #endif
 }
 BPC_FI int clz32(uint32_t x) {
@@ -524,7 +524,7 @@ struct Coder {
     template <int PK, int H>
     BPC_FI void dec_ctx_half(uint32_t u, int b, bool act) {
         while (u) {
-            const int j = ctz64(u);
+            const int j = ctz32(u);
             u &= u - 1;
             ring_ensure<4>();  // one row: two steps of up to two AC calls
             dec_ctx_step<PK, H, 0>(j, 0, b, act);
@@ -559,7 +559,7 @@ struct Coder {
     template <int H>
     BPC_FI void dec_mrp_half(uint32_t u, int b, bool act, uint32_t P) {
         while (u) {
-            const int j = ctz64(u);
+            const int j = ctz32(u);
             u &= u - 1;
             ring_ensure<2>();  // one row: two steps of one AC call
             dec_mrp_step<H>(j, 0, b, act, P);
@@ -873,7 +873,7 @@ struct Coder {
                 gq = zip16(sg[0], sg[1], q);
             }
             do {
-                const int t = ctz64(kq);
+                const int t = ctz32(kq);
                 kq &= kq - 1;
                 const int key = (32 * q + t) * 2;  // (row, column, phase) in the pass
                 if (PK == PK_MRP) {
