@@ -175,7 +175,7 @@ bool order_pays(bool enc, int ncb, int cbs) {
     const int ng = cbs == 64 ? 1 : 2;
     // an image within two waves gains nothing: every unit starts at once or
     // in the second wave anyway, and the planning kernels cost more
-    return (ncb + ng - 1) / ng >= 2 * resident_warps(enc);
+    return (long long)((ncb + ng - 1) / ng) >= 2LL * resident_warps(enc);
 }
 
 cudaError_t plan_order(bool enc, int cbs, const Params &p, int *sched, cudaStream_t st, const int **order) {
