@@ -21,6 +21,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <atomic>
+
 #include "bpc_kernels.h"
 
 namespace bpc {
@@ -136,13 +138,18 @@ __global__ void __launch_bounds__(kBuckets) k_order(const uint32_t *key, int uni
     }
 }
 
+// warps resident at once on the current device (SM count cached per device;
+// callers may be on any host thread)
 int resident_warps(bool enc) {
-    static int sms[64] = {};
+    static std::atomic<int> sms[64];
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 1 << 30;
-    if (!sms[dev] && cudaDeviceGetAttribute(&sms[dev], cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
-        return 1 << 30;
-    return sms[dev] * kWarps * (enc ? kMinCtasEnc : kMinCtasDec);
+    int n = sms[dev].load(std::memory_order_relaxed);
+    if (!n) {
+        if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) return 1 << 30;
+        sms[dev].store(n, std::memory_order_relaxed);
+    }
+    return n * kWarps * (enc ? kMinCtasEnc : kMinCtasDec);
 }
 
 template <int CBS>
