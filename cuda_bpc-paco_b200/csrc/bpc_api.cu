@@ -54,10 +54,11 @@ bool valid_geometry(int X, int Y, int cb, int levels) {
     return true;
 }
 
-int fill_params(bpc::Params &p, const int *in, int *out, int X, int Y, const int *d_lut, int lut_n, int passes,
-                int levels, int cb, int *d_status, int *d_counts) {
+int fill_params(bpc::Params &p, bool enc, const int *in, int *out, int X, int Y, const int *d_lut, int lut_n,
+                int passes, int levels, int cb, int *d_status, int *d_counts) {
     if (!valid_mode(passes, levels, cb) || !valid_geometry(X, Y, cb, levels) || !in || !out || !d_lut || lut_n <= 0)
         return BPC_ERR_ARG;
+    if (!bpc::aligned_to(in, enc ? bpc::kEncInAlign : bpc::kDecInAlign)) return BPC_ERR_ARG;
     const bpc::LutOffsets o = bpc::lut_offsets(levels, passes, lut_n);
     p.in = in;
     p.out = out;
@@ -84,7 +85,7 @@ int code_device(bool enc, const int *in, int *out, int X, int Y, const int *d_lu
                 int cb, int *d_status, int *d_counts, int grid, void *stream, int cb_begin = 0, int cb_end = -1,
                 int *sched = nullptr) {
     bpc::Params p;
-    const int rc = fill_params(p, in, out, X, Y, d_lut, lut_n, passes, levels, cb, d_status, d_counts);
+    const int rc = fill_params(p, enc, in, out, X, Y, d_lut, lut_n, passes, levels, cb, d_status, d_counts);
     if (rc) return rc;
     if (cb_end >= 0) {
         p.cb_begin = cb_begin;

@@ -40,6 +40,7 @@ struct BatchImage {
     int X, Y, levels, cbs, ncbx, ncb;
     int a_sig, a_sign, cp_off;
     long long cb_base;
+    long long in_words;  // decode: words of the compact container (offsets must stay inside it)
 };
 
 struct BatchItem {
@@ -131,6 +132,7 @@ __global__ void __launch_bounds__(kWarps * 32, ENC ? kMinCtasEnc : kMinCtasDec)
         p.status = status;
         p.counts = counts ? counts + im.cb_base : nullptr;
         p.offsets = offsets ? offsets + im.cb_base : nullptr;
+        p.in_words = im.in_words;
         p.cb_begin = 0;
         p.cb_end = im.ncb;
         for (int k = 0; k < item.n; k += G::NG) {
@@ -533,7 +535,7 @@ int bpc_batch_encode(void *batch, const int *const *d_coeffs, int *d_compact, lo
     if (!b || !d_coeffs || !d_compact || !d_offsets) return BPC_ERR_ARG;
     std::vector<BatchImage> h(b->n);
     for (int i = 0; i < b->n; i++) {
-        if (!d_coeffs[i]) return BPC_ERR_ARG;
+        if (!d_coeffs[i] || !bpc::aligned_to(d_coeffs[i], bpc::kEncInAlign)) return BPC_ERR_ARG;
         image_desc(*b, i, h[i]);
         h[i].in = d_coeffs[i];
         h[i].out = b->slots[i];
@@ -550,6 +552,7 @@ int bpc_batch_decode(void *batch, const int *d_compact, const long long *d_offse
         if (!d_coeffs[i]) return BPC_ERR_ARG;
         image_desc(*b, i, h[i]);
         h[i].in = d_compact;
+        h[i].in_words = b->words;
         h[i].out = d_coeffs[i];
     }
     return run(*b, false, h.data(), nullptr, d_offsets, nullptr, d_status, (cudaStream_t)stream);

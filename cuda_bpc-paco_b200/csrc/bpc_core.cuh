@@ -82,6 +82,7 @@ struct Params {
     // decoder input in the compact container: codeblock k's words (MSB and
     // codewords) are in[offsets[k] .. offsets[k+1]); null = slot layout
     const long long *offsets;
+    long long in_words = 0;  // compact container: its length in words (offsets outside it are damage)
     int cb_begin, cb_end;  // codeblocks [cb_begin, cb_end) of the image are coded by this launch
     // work order of a whole-image launch: warp slot k codes the codeblocks
     // starting at order[k] (null = raster order)
@@ -1049,9 +1050,12 @@ struct Coder {
         } else {
             if (p.offsets) {  // compact container; words past the codeblock read as the -1 fill
                 const long long o0 = ok ? p.offsets[cb] : 0, o1 = ok ? p.offsets[cb + 1] : 0;
-                slot_in = p.in + o0;
-                const long long n = o1 - o0;
-                in_cap = (uint32_t)(n < 0 ? 0 : (n > (long long)cap ? (long long)cap : n));
+                // damaged offsets (outside the container, or decreasing) read
+                // nothing: the codeblock then decodes as a bad stream
+                const bool inside = o0 >= 0 && o1 >= o0 && o1 <= p.in_words;
+                slot_in = p.in + (inside ? o0 : 0);
+                const long long n = inside ? o1 - o0 : 0;
+                in_cap = (uint32_t)(n > (long long)cap ? (long long)cap : n);
             } else {
                 slot_in = p.in + (ok ? (size_t)cb * cap : 0);
                 in_cap = (uint32_t)cap;

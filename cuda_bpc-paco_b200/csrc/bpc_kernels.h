@@ -22,6 +22,13 @@ constexpr int kWarps = 4;  // warps (codeblocks) per CTA
 constexpr int kMinCtasDec = DEC_MIN_CTAS;
 constexpr int kMinCtasEnc = ENC_MIN_CTAS;
 
+// Input alignment the kernels' vector loads need: the encoder reads each
+// lane's two coefficients with one 8-byte load, the decoder reads the slot
+// stream with 16-byte loads.  Entry points refuse other pointers (a misaligned
+// vector load would fault and lose the CUDA context).
+constexpr unsigned kEncInAlign = 8, kDecInAlign = 16;
+inline bool aligned_to(const void *p, unsigned a) { return ((uintptr_t)p & (uintptr_t)(a - 1)) == 0; }
+
 // Launch the encoder (enc) or decoder over p.ncb codeblocks.  grid <= 0 picks
 // one CTA per kWarps codeblocks; a positive grid runs persistent CTAs that
 // walk the codeblocks grid-stride.
@@ -32,7 +39,8 @@ cudaError_t launch_code(bool enc, int passes, int cbs, const Params &p, int grid
 // the image's work units by expected cost and set *order to the order to put
 // in Params; *order stays null (raster order) for images of at most two waves.
 long long sched_ints(int ncb, int cbs);
-bool order_pays(bool enc, int ncb, int cbs);  // more than two waves on this device
+// more than two waves on device `dev` (-1: the current device)
+bool order_pays(bool enc, int ncb, int cbs, int dev = -1);
 cudaError_t plan_order(bool enc, int cbs, const Params &p, int *sched, cudaStream_t st, const int **order);
 
 // LUT training: add, per LUT entry, [2k] symbols coded and [2k+1] symbols

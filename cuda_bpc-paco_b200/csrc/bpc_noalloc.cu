@@ -29,8 +29,12 @@
 // its device address; passing the name to a kernel would fault or, where the
 // GPU can reach host memory, silently use the wrong memory.  So the first call
 // on each device (with that device current) looks the device address up with
-// cudaGetSymbolAddress and keeps it; make that first call before any stream
-// capture begins.
+// cudaGetSymbolAddress and keeps it, together with the CUDA context it belongs
+// to; make that first call before any stream capture begins.  A kept address
+// is only valid in its context: after cudaDeviceReset (or any other change of
+// the device's current context) the next call sees a different context and
+// looks the address up again, which makes that call a set-up call too.
+#include <cuda.h>  // CUcontext; cuCtxGetCurrent itself comes from the runtime's entry-point query
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -57,6 +61,24 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 constexpr int kMaxDevices = 64;
 std::mutex g_mu;
 unsigned char *g_addr[kMaxDevices] = {};
+CUcontext g_ctx[kMaxDevices] = {};
+
+// the calling thread's current CUDA context (null if none yet, or if the
+// driver entry point cannot be found)
+CUcontext current_context() {
+    using Fn = CUresult (*)(CUcontext *);
+    static const Fn fn = [] {
+        void *f = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            f = nullptr;
+        return (Fn)f;
+    }();
+    CUcontext c = nullptr;
+    if (!fn || fn(&c) != CUDA_SUCCESS) return nullptr;
+    return c;
+}
 
 // container words per codeblock: MSB + codewords, capped at the slot size
 __global__ void k_noalloc_sizes(const int *counts, long long ncb, long long cap, long long *sizes) {
@@ -79,13 +101,15 @@ __global__ void k_noalloc_gather(const int32_t *slots, long long cap, const long
     }
 }
 
-// device address of the array on the current device (looked up once per device)
+// device address of the array on the current device (looked up once per
+// device and context)
 int scratch_address(unsigned char **out) {
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess || dev < 0 || dev >= kMaxDevices) return BPC_ERR_CUDA;
     std::lock_guard<std::mutex> g(g_mu);
-    if (!g_addr[dev]) {
+    const CUcontext ctx = current_context();
+    if (!g_addr[dev] || !ctx || ctx != g_ctx[dev]) {
         void *p = nullptr;
         e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
         if (e != cudaSuccess || !p) {
@@ -99,6 +123,7 @@ int scratch_address(unsigned char **out) {
             return BPC_ERR_CUDA;
         }
         g_addr[dev] = (unsigned char *)p;
+        g_ctx[dev] = current_context();  // the lookup made the device's context current
     }
     *out = g_addr[dev];
     return BPC_OK;
@@ -111,7 +136,7 @@ extern "C" int bpc_encode_compact_noalloc(const int *d_coeffs, int X, int Y, con
                                           int *d_status, void *stream) {
     if (!d_coeffs || !d_lut || lut_n <= 0 || !d_compact || !d_offsets || (passes != 2 && passes != 3) ||
         (cb_size != 64 && cb_size != 32) || levels < 1 || levels > 16 || X <= 0 || Y <= 0 || X % cb_size ||
-        Y % cb_size)
+        Y % cb_size || !bpc::aligned_to(d_coeffs, bpc::kEncInAlign))
         return BPC_ERR_ARG;
     if ((long long)X * (long long)Y > kMaxWords) {
         std::fprintf(stderr, "bpc: %d x %d exceeds the %lld coefficients of the no-allocation entry point\n", X, Y,

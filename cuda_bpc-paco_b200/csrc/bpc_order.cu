@@ -138,12 +138,12 @@ __global__ void __launch_bounds__(kBuckets) k_order(const uint32_t *key, int uni
     }
 }
 
-// warps resident at once on the current device (SM count cached per device;
-// callers may be on any host thread)
-int resident_warps(bool enc) {
+// warps resident at once on device `dev` (-1: the current device; SM count
+// cached per device; callers may be on any host thread)
+int resident_warps(bool enc, int dev) {
     static std::atomic<int> sms[64];
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 1 << 30;
+    if (dev < 0 && cudaGetDevice(&dev) != cudaSuccess) return 1 << 30;
+    if (dev < 0 || dev >= 64) return 1 << 30;
     int n = sms[dev].load(std::memory_order_relaxed);
     if (!n) {
         if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) return 1 << 30;
@@ -178,11 +178,11 @@ long long sched_ints(int ncb, int cbs) {
     return 2LL * ((ncb + ng - 1) / ng);
 }
 
-bool order_pays(bool enc, int ncb, int cbs) {
+bool order_pays(bool enc, int ncb, int cbs, int dev) {
     const int ng = cbs == 64 ? 1 : 2;
     // an image within two waves gains nothing: every unit starts at once or
     // in the second wave anyway, and the planning kernels cost more
-    return (long long)((ncb + ng - 1) / ng) >= 2LL * resident_warps(enc);
+    return (long long)((ncb + ng - 1) / ng) >= 2LL * resident_warps(enc, dev);
 }
 
 cudaError_t plan_order(bool enc, int cbs, const Params &p, int *sched, cudaStream_t st, const int **order) {

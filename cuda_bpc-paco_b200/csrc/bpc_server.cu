@@ -266,12 +266,15 @@ extern "C" long long bpc_server_submit(void *srv, int direction, const int *d_in
                                        int cb_size) {
     Server *s = as_server(srv);
     if (!s || !d_in || (direction != BPC_CODE && direction != BPC_DECODE) || (cb_size != 64 && cb_size != 32) ||
-        X <= 0 || Y <= 0 || X % cb_size || Y % cb_size)
+        X <= 0 || Y <= 0 || X % cb_size || Y % cb_size ||
+        !bpc::aligned_to(d_in, direction == BPC_CODE ? bpc::kEncInAlign : bpc::kDecInAlign))
         return BPC_ERR_ARG;
     size_t bytes = ((size_t)X * (size_t)Y * sizeof(int) + kAlign - 1) / kAlign * kAlign;
     size_t sched_off = 0;
     const int ncb = (X / cb_size) * (Y / cb_size);
-    if (bpc::order_pays(direction == BPC_CODE, ncb, cb_size)) {  // large request: work-ordered coding
+    // decided for the server's device, as the worker thread (which has that
+    // device current) decides again when it launches the request
+    if (bpc::order_pays(direction == BPC_CODE, ncb, cb_size, s->device)) {  // large request: work-ordered coding
         sched_off = bytes;
         bytes += ((size_t)bpc::sched_ints(ncb, cb_size) * sizeof(int) + kAlign - 1) / kAlign * kAlign;
     }

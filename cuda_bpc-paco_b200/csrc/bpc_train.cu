@@ -39,7 +39,7 @@ extern "C" int bpc_lut_stats(const int *d_coeffs, int X, int Y, int passes, int 
                              unsigned long long *d_stats, void *stream) {
     if (!d_coeffs || !d_stats || (passes != 2 && passes != 3) || levels < 1 || levels > 16 ||
         (cb_size != 64 && cb_size != 32) || X <= 0 || Y <= 0 || X % cb_size || Y % cb_size ||
-        (long long)X * Y > (1LL << 31) - 1)
+        (long long)X * Y > (1LL << 31) - 1 || !bpc::aligned_to(d_coeffs, bpc::kEncInAlign))
         return BPC_ERR_ARG;
     const int n = bpc_lut_entries(passes, levels, kPlanes);
     const bpc::LutOffsets o = bpc::lut_offsets(levels, passes, n);

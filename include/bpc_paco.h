@@ -105,6 +105,14 @@ int bpc_host_band_rows(int X, int Y, int cb_size, int *starts, int capacity);
 
 /* ---------------------------------------------------------------------------
  * Device-pointer entry points: stream-ordered, no allocation, no host sync.
+ *
+ * Alignment: the kernels read coefficients with 8-byte loads and slot streams
+ * with 16-byte loads, so every device input that is a coefficient image
+ * (encode, LUT statistics, batch encode, server encode requests) must be
+ * 8-byte aligned and every slot-stream input (decode, server decode requests)
+ * 16-byte aligned; other pointers are refused with BPC_ERR_ARG before anything
+ * is launched.  cudaMalloc'd buffers, and offsets into them by whole
+ * codeblock rows, always qualify.
  * ------------------------------------------------------------------------- */
 
 /* Encode X x Y raster coefficients (device) into the slot stream (device,
@@ -174,8 +182,11 @@ int bpc_batch_destroy(void *batch);
  * BPC_ERR_TOO_LARGE.  Output as bpc_batch_encode for a one-image batch:
  * d_compact (at most X*Y ints) and d_offsets (codeblocks + 1 entries).  The
  * first call on each device looks the array's device address up; make that
- * call before any stream capture.  All calls share the array: calls that
- * overlap on the GPU race, so serialise them. */
+ * call before any stream capture.  The address is kept per device and CUDA
+ * context: after cudaDeviceReset the next call sees a new context and looks it
+ * up again (so that call is a first call too).  All calls share the array:
+ * calls that overlap on the GPU race, so serialise them.  d_coeffs must be
+ * 8-byte aligned (BPC_ERR_ARG otherwise). */
 int bpc_encode_compact_noalloc(const int *d_coeffs, int X, int Y, const int *d_lut, int lut_n, int passes, int levels,
                                int cb_size, int *d_compact, long long *d_offsets, int *d_status, void *stream);
 

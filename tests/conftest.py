@@ -9,7 +9,8 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 PKG = os.path.join(ROOT, "cuda_bpc-paco_b200")
 GOLDEN = os.path.join(ROOT, "tests", "golden")
 LUTS = os.path.join(GOLDEN, "luts")
-REF_ROOT = "/root/reference"  # only read by CPU tests, which skip without it
+# the reference checkout (BPC_REFERENCE_DIR); only read by CPU tests, which skip without it
+REF_ROOT = os.environ.get("BPC_REFERENCE_DIR", "/root/reference")
 
 for p in (PKG, os.path.join(ROOT, "oracle"), GOLDEN):
     if p not in sys.path:

@@ -211,6 +211,7 @@ extern "C" int emu_code(int enc, int kind, int passes, int cbs, const int32_t *i
     p.status = &status;
     p.counts = nullptr;
     p.offsets = enc ? nullptr : offsets;  // decode from the compact container when given
+    p.in_words = (long long)X * Y;       // the container lies in the X*Y-word input buffer
     p.cb_begin = 0;
     p.cb_end = p.ncb;
     int rc;

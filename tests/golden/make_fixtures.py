@@ -139,4 +139,4 @@ def sample_image_full(ref_root: str) -> np.ndarray:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    main(sys.argv[1] if len(sys.argv) > 1 else os.environ.get("BPC_REFERENCE_DIR", "/root/reference"))

@@ -145,3 +145,20 @@ def test_device_entry_points_reject_bad_geometry(bpc):
         assert rc == bpc.ERR_ARG
     assert L.bpc_decode_device(vp(16), vp(16), 64, 64, None, 3360, 2, 5, 64, None, None, 0, None) == bpc.ERR_ARG
     assert L.bpc_encode_device(vp(16), vp(16), 64, 64, vp(16), 3360, 4, 5, 64, None, None, 0, None) == bpc.ERR_ARG
+
+
+def test_device_entry_points_reject_misaligned_inputs(bpc):
+    """Coefficient inputs need 8-byte and slot-stream inputs 16-byte alignment
+    (the kernels' vector loads); other pointers are refused before any CUDA
+    call, valid geometry or not."""
+    vp = ctypes.c_void_p
+    L = bpc.lib()
+    args = (64, 64, vp(4096), 3360, 2, 5, 64, None, None, 0, None)
+    assert L.bpc_encode_device(vp(4096 + 4), vp(4096), *args) == bpc.ERR_ARG
+    assert L.bpc_decode_device(vp(4096 + 8), vp(4096), *args) == bpc.ERR_ARG
+    sargs = (64, 64, vp(4096), 3360, 2, 5, 64, None, None, vp(4096), None)
+    assert L.bpc_encode_device_sched(vp(4096 + 4), vp(4096), *sargs) == bpc.ERR_ARG
+    assert L.bpc_decode_device_sched(vp(4096 + 8), vp(4096), *sargs) == bpc.ERR_ARG
+    assert L.bpc_encode_compact_noalloc(vp(4096 + 4), 64, 64, vp(4096), 3360, 2, 5, 64, vp(4096), vp(4096), None,
+                                        None) == bpc.ERR_ARG
+    assert L.bpc_lut_stats(vp(4096 + 4), 64, 64, 2, 5, 64, vp(4096), None) == bpc.ERR_ARG

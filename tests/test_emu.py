@@ -102,3 +102,31 @@ def test_decode_from_compact_container(emu, oracle_mod, passes, cb):
     buf[:compact.size] = compact
     dec, _ = run(emu, 0, buf, img.shape, lut, passes, 5, cb, offsets=offsets)
     np.testing.assert_array_equal(dec.reshape(img.shape), img)
+
+
+def test_compact_container_damaged_offsets(emu, oracle_mod):
+    """Offsets that point outside the container, or decrease, are damage: the
+    codeblock decodes as a bad stream (zeros, status bit 2) without reading
+    outside the container, and the other codeblocks decode intact."""
+    img = bpc_synth.synthetic_coefficients(128, 5, 13, amp=30)
+    lut = oracle_mod.load_luts(lut_folder(3), 3, 5)
+    slots = oracle_mod.encode(img, lut, 3, 5, 64).reshape(-1, 64 * 64)
+    sizes = np.minimum((slots[:, 1:] != -1).sum(1) + 1, 64 * 64)
+    offsets = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int64)
+    compact = np.concatenate([slots[g, :sizes[g]] for g in range(len(sizes))]).astype(np.int32)
+    buf = np.zeros(img.size, np.int32)
+    buf[:compact.size] = compact
+    bad = offsets.copy()
+    bad[3] = img.size + 10**9       # codeblock 2 ends, codeblock 3 starts, past the container
+    dec, st = run(emu, 0, buf, img.shape, lut, 3, 5, 64, offsets=bad)
+    assert st & 2
+    blocks = dec.reshape(2, 64, 2, 64).transpose(0, 2, 1, 3).reshape(4, 64, 64)
+    want = img.reshape(2, 64, 2, 64).transpose(0, 2, 1, 3).reshape(4, 64, 64)
+    np.testing.assert_array_equal(blocks[:2], want[:2])
+    assert not blocks[2].any() and not blocks[3].any()
+    bad = offsets.copy()
+    bad[1] = -5                     # negative start
+    dec, st = run(emu, 0, buf, img.shape, lut, 3, 5, 64, offsets=bad)
+    assert st & 2
+    blocks = dec.reshape(2, 64, 2, 64).transpose(0, 2, 1, 3).reshape(4, 64, 64)
+    np.testing.assert_array_equal(blocks[2:], want[2:])
