@@ -47,9 +47,58 @@ CONFIGS = {
     "cfg5l": dict(side=16384, levels=5, passes=3, cb=64, laplacian=True, gpu_input=True),
 }
 METRIC = "encode/decode Gcoeff/s (bit-exact)"
-# DRAM read + write bytes of one launch of the dominant kernel (the decoder),
-# from the ncu capture summarised in profiles/k_bpc_cfg2_full.md.
-NCU_TRAFFIC = {"cfg2": 15.08992e6 + 18.553856e6}
+# ncu counters of the coder kernels per workload, written by
+# `python bench.py --ncu-import <raw csv> --workload <name>` from a capture of
+# this source (see the header of the file for the capture command)
+COUNTERS = os.path.join(ROOT, "profiles", "k_bpc_counters.txt")
+
+
+def load_counters():
+    """{(workload, kernel): {launches, time_us, dram_read, dram_write, warp_inst}}"""
+    out = {}
+    try:
+        with open(COUNTERS) as f:
+            for line in f:
+                t = line.split()
+                if not t or t[0].startswith("#") or len(t) < 7:
+                    continue
+                out[(t[0], t[1])] = {"launches": int(t[2]), "time_us": float(t[3]), "dram_read": float(t[4]),
+                                     "dram_write": float(t[5]), "warp_inst": float(t[6])}
+    except OSError:
+        pass
+    return out
+
+
+def ncu_import(path, workload):
+    """Lines for COUNTERS from `ncu -i <rep> --page raw --csv` output: per
+    coder kernel (encoder / decoder) the mean over its captured launches."""
+    import csv
+    rows = list(csv.reader(open(path)))
+    hdr = next(i for i, r in enumerate(rows) if "Kernel Name" in r)
+    names, units = rows[hdr], rows[hdr + 1]
+    col = {n: i for i, n in enumerate(names)}
+    scale = {"byte": 1, "Kbyte": 1e3, "Mbyte": 1e6, "Gbyte": 1e9, "KB": 1e3, "MB": 1e6, "GB": 1e9,
+             "nsecond": 1e-3, "usecond": 1.0, "msecond": 1e3, "inst": 1, "Kinst": 1e3, "Minst": 1e6,
+             "Ginst": 1e9, "": 1}
+
+    def val(r, m):
+        i = col[m]
+        return float(r[i].replace(",", "")) * scale.get(units[i], 1)
+
+    acc = {}
+    for r in rows[hdr + 2:]:
+        if len(r) != len(names) or "k_bpc" not in r[col["Kernel Name"]] or "batch" in r[col["Kernel Name"]]:
+            continue
+        kname = r[col["Kernel Name"]]
+        kind = "encoder" if ("1>" in kname or "true>" in kname) else "decoder"
+        a = acc.setdefault(kind, [0, 0.0, 0.0, 0.0, 0.0])
+        a[0] += 1
+        a[1] += val(r, "gpu__time_duration.sum")
+        a[2] += val(r, "dram__bytes_read.sum")
+        a[3] += val(r, "dram__bytes_write.sum")
+        a[4] += val(r, "smsp__inst_executed.sum")
+    for kind, (n, t, rd, wr, ins) in sorted(acc.items()):
+        print(f"{workload} {kind} {n} {t / n:.1f} {rd / n:.0f} {wr / n:.0f} {ins / n:.0f}")
 
 
 def workload_name(c):
@@ -74,6 +123,37 @@ def load_peaks():
             return float(json.load(f)["hbm_gbs"]), "measured"
     except Exception:
         return 6650.0, "fallback"
+
+
+def bench_config(args, c, world):
+    """The workload both arms report (same keys and values)."""
+    return {"workload": workload_name(c), "name": args.config, "coefficients_per_gpu": c["side"] * c["side"],
+            "l2": "GPU kernels: L2 flushed (256 MiB write) before every kernel; inputs of 4 B per coefficient",
+            "parallelism": f"replicas x{world}"}
+
+
+def copy_floor(n_words, dev, reps=5):
+    """Seconds for one encode+decode step's PCIe traffic alone: per call X*Y
+    int32 host -> device and X*Y int32 device -> host from pinned memory,
+    both directions at once on two streams (the host-buffer calls overlap
+    them), twice (encode call + decode call).  Median of `reps`."""
+    import torch
+    h_in = torch.empty(n_words, dtype=torch.int32, pin_memory=True)
+    h_out = torch.empty(n_words, dtype=torch.int32, pin_memory=True)
+    d_a = torch.empty(n_words, dtype=torch.int32, device=dev)
+    d_b = torch.empty(n_words, dtype=torch.int32, device=dev)
+    s1, s2 = torch.cuda.Stream(dev), torch.cuda.Stream(dev)
+    ts = []
+    for _ in range(reps + 1):
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        with torch.cuda.stream(s1):
+            d_a.copy_(h_in, non_blocking=True)
+        with torch.cuda.stream(s2):
+            h_out.copy_(d_b, non_blocking=True)
+        torch.cuda.synchronize(dev)
+        ts.append(time.perf_counter() - t0)
+    return 2 * float(np.median(ts[1:]))
 
 
 class ClockSampler:
@@ -220,7 +300,7 @@ def run_reference(args, c):
         "impl": "reference", "metric": METRIC, "value": v, "unit": "Gcoeff/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(times) / len(times),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
-        "data": "synthetic", "config": {"workload": workload_name(c), "l2": "n/a (CPU)"},
+        "data": "synthetic", "config": bench_config(args, c, world),
         "cpu_baseline": {"value": v, "unit": "Gcoeff/s", "cores": threads, "kind": "port", "sample": sample},
         "e2e": {"value": v, "unit": "Gcoeff/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }))
@@ -581,6 +661,13 @@ def run_ours(args, c):
         tdist.barrier()
     torch.cuda.synchronize()
     with ClockSampler(local if dist else 0) as clk:
+        # the sampler polls every 50 ms: keep the GPU busy for a moment
+        # before the timed region so that samples under load exist
+        t_pre = time.perf_counter()
+        while time.perf_counter() - t_pre < 0.3:
+            step()
+            torch.cuda.synchronize()
+        torch.cuda.synchronize()
         w0 = time.perf_counter()
         for _ in range(args.steps):
             step(times)
@@ -628,30 +715,59 @@ def run_ours(args, c):
     e2e_step = float(np.mean(e2e_t))
     e2e_step = max_over_ranks(e2e_step, dev)
     e2e = 2 * N * world / e2e_step / 1e9
+    floor = max_over_ranks(copy_floor(N, dev), dev)
 
     peak, peak_kind = load_peaks()
     alg_bytes = 8.0 * N  # per launch: 4 B/coef in + 4 B/coef out (slot stream), encode and decode alike
     te1, td1 = te / args.steps, td / args.steps
     dom_t = max(te1, td1)
+    dom = "decoder" if td1 >= te1 else "encoder"
     achieved = alg_bytes / dom_t / 1e9
+    clocks = clk.summary()
+    # issue roofline: warp instructions of one launch of the dominant kernel
+    # (ncu capture of this workload) over what the SMs can issue in the
+    # launch's CUDA-event time at the clock sampled during the run
+    cnt = load_counters().get((args.config, dom))
+    sms = torch.cuda.get_device_properties(dev).multi_processor_count
+    mhz = clocks.get("sm_mhz") or clocks.get("sm_max_mhz")
+    issue = None
+    if cnt and mhz:
+        peak_inst = sms * 4 * mhz * 1e6  # one warp instruction per SM sub-partition per cycle
+        issue = {"warp_inst_per_launch": cnt["warp_inst"], "achieved_ginst_s": cnt["warp_inst"] / dom_t / 1e9,
+                 "peak_ginst_s": peak_inst / 1e9, "frac": cnt["warp_inst"] / dom_t / peak_inst, "sm_mhz": mhz,
+                 "sms": sms, "source": "profiles/k_bpc_counters.txt"}
     line = {
         "metric": METRIC, "value": value, "unit": "Gcoeff/s", "n_gpus": world, "steps": args.steps,
         "warmup": max(args.warmup, 3), "ms_per_step": 1e3 * t_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded generator + 5/3 DWT)",
-        "config": {"workload": workload_name(c), "name": args.config, "coefficients_per_gpu": N,
-                   "l2": "flushed (256 MiB write) before every kernel", "parallelism": f"replicas x{world}"},
+        "config": bench_config(args, c, world),
         "encode_gcoeffs": N / te1 / 1e9, "decode_gcoeffs": N / td1 / 1e9,
-        "e2e": {"value": e2e, "unit": "Gcoeff/s", "h2d_bytes_per_step": 2 * 4 * N, "d2h_bytes_per_step": 2 * 4 * N + 8},
+        "encode_ms": 1e3 * te1, "decode_ms": 1e3 * td1,
+        "e2e": {"value": e2e, "unit": "Gcoeff/s", "h2d_bytes_per_step": 2 * 4 * N, "d2h_bytes_per_step": 2 * 4 * N + 8,
+                "ms_per_step": 1e3 * e2e_step, "copy_floor_ms": 1e3 * floor, "frac_of_floor": floor / e2e_step,
+                "copy_floor": "pinned H2D + D2H of X*Y int32 each, both directions at once, per call, x2 calls"},
         "gpu_launches": args.steps * (launches_per_call(X, Y, cb, True, dev) + launches_per_call(X, Y, cb, False, dev)),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": NCU_TRAFFIC.get(args.config), "peak_source": peak_kind,
-                     "kernel": "k_bpc decoder" if td1 >= te1 else "k_bpc encoder",
-                     "note": "8 B/coefficient algorithmic; the coder is bound by SM integer issue, not HBM"},
-        "clocks": clk.summary(), "wall_s_timed": wall,
+                     "traffic": (cnt["dram_read"] + cnt["dram_write"]) if cnt else None, "peak_source": peak_kind,
+                     "kernel": f"k_bpc {dom}", "issue": issue,
+                     "note": "8 B/coefficient algorithmic; the coder is bound by SM integer issue and by the serial "
+                             "chain of its heaviest codeblocks, not HBM; traffic and warp_inst from the ncu capture "
+                             "of this workload (profiles/k_bpc_counters.txt)"},
+        "clocks": clocks, "wall_s_timed": wall,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        # baselines, after the timed region: the CPU restatement on the host
+        # cores and the reference kernel rebuilt for this GPU (the timing bar)
         lut_np = bpc.load_luts_host(os.path.join(LUT_DIR, f"{passes}_coding_pass"), passes, levels)
         line["cpu_baseline"] = cpu_baseline(img, lut_np, c)
+        if not args.no_ref_kernel:
+            import time_ref
+            rk = time_ref.time_reference_kernel(c, img, steps=min(args.steps, 10), warmup=3, flush=flush)
+            line["ref_kernel"] = rk
+            if "gcoeffs" in rk:
+                line["vs_ref_kernel"] = value / rk["gcoeffs"]
+                line["vs_ref_kernel_by_direction"] = {"encode": line["encode_gcoeffs"] / rk["encode_gcoeffs"],
+                                                      "decode": line["decode_gcoeffs"] / rk["decode_gcoeffs"]}
     lut.close()
     if dist:
         tdist.barrier()
@@ -786,7 +902,13 @@ def main():
     ap.add_argument("--budget-gb", type=float, default=120.0, help="cfg4: HBM admission budget")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="kernel timing only (profiling runs)")
+    ap.add_argument("--no-ref-kernel", action="store_true", help="skip timing the rebuilt reference kernel")
+    ap.add_argument("--ncu-import", help="print counter lines for profiles/k_bpc_counters.txt from ncu raw csv")
+    ap.add_argument("--workload", default="cfg2", help="--ncu-import: workload name of the capture")
     args = ap.parse_args()
+    if args.ncu_import:
+        ncu_import(args.ncu_import, args.workload)
+        return
     if args.config in ("dwt", "train") and args.impl == "ours":
         (run_dwt if args.config == "dwt" else run_train)(args)
         return

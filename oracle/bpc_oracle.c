@@ -556,6 +556,7 @@ typedef struct {
     int32_t *status; /* per codeblock, may be NULL */
     int ref_quirk;
     long ncb, next;
+    const long *list; /* if not NULL: work item k is codeblock list[k] */
     pthread_mutex_t mu;
     int any_status;
     uint64_t *stats; /* LUT training counts (summed over the workers), or NULL */
@@ -698,8 +699,9 @@ static void *worker(void *p) {
         if (k >= j->ncb) break;
         long e = k + chunk < j->ncb ? k + chunk : j->ncb;
         for (; k < e; k++) {
-            int st = a->enc ? encode_block(c, j, k) : decode_block(c, j, k);
-            if (j->status) j->status[k] = st;
+            const long g = j->list ? j->list[k] : k;
+            int st = a->enc ? encode_block(c, j, g) : decode_block(c, j, g);
+            if (j->status) j->status[g] = st;
             st_all |= st;
         }
     }
@@ -715,7 +717,7 @@ static void *worker(void *p) {
 
 static int run(int enc, const int32_t *in, int32_t *out, int X, int Y, const int *lut, int lut_n, int passes,
                int levels, int cb, int nthreads, int32_t *status, int ref_quirk, long cb_begin, long cb_end,
-               uint64_t *stats, long stats_n) {
+               uint64_t *stats, long stats_n, const long *list) {
     if (!in || !out || !lut || X <= 0 || Y <= 0 || (passes != 2 && passes != 3) || levels < 1 ||
         (cb != 64 && cb != 32) || X % cb || Y % cb)
         return BPCO_ERR_ARG;
@@ -735,10 +737,17 @@ static int run(int enc, const int32_t *in, int32_t *out, int X, int Y, const int
     j.stats = stats;
     j.stats_n = stats_n;
     long ncb = (long)(X / cb) * (Y / cb);
+    if (list) { /* cb_end = list length; every entry must name a codeblock */
+        for (long k = 0; k < cb_end; k++)
+            if (list[k] < 0 || list[k] >= ncb) return BPCO_ERR_ARG;
+        ncb = cb_end;
+        cb_begin = 0;
+    }
     if (cb_end < 0 || cb_end > ncb) cb_end = ncb;
     if (cb_begin < 0) cb_begin = 0;
     j.ncb = cb_end;
     j.next = cb_begin;
+    j.list = list;
     pthread_mutex_init(&j.mu, NULL);
     if (nthreads < 1) nthreads = 1;
     if (nthreads > 256) nthreads = 256;
@@ -755,13 +764,27 @@ static int run(int enc, const int32_t *in, int32_t *out, int X, int Y, const int
  * Returns the OR of the per-codeblock status bits, or a negative error. */
 int bpco_encode(const int32_t *img, int32_t *stream, int X, int Y, const int *lut, int lut_n, int passes, int levels,
                 int cb, int nthreads, int32_t *status, long cb_begin, long cb_end) {
-    return run(1, img, stream, X, Y, lut, lut_n, passes, levels, cb, nthreads, status, 0, cb_begin, cb_end, NULL, 0);
+    return run(1, img, stream, X, Y, lut, lut_n, passes, levels, cb, nthreads, status, 0, cb_begin, cb_end, NULL, 0,
+               NULL);
 }
 
 int bpco_decode(const int32_t *stream, int32_t *img, int X, int Y, const int *lut, int lut_n, int passes, int levels,
                 int cb, int nthreads, int32_t *status, int ref_quirk, long cb_begin, long cb_end) {
     return run(0, stream, img, X, Y, lut, lut_n, passes, levels, cb, nthreads, status, ref_quirk, cb_begin,
-               cb_end, NULL, 0);
+               cb_end, NULL, 0, NULL);
+}
+
+/* bpco_encode / bpco_decode over the n codeblocks listed in `list` (indices in
+ * raster order of codeblocks), for spot checks of images too large to code
+ * whole; the slots and pixels of other codeblocks are left as they are. */
+int bpco_encode_list(const int32_t *img, int32_t *stream, int X, int Y, const int *lut, int lut_n, int passes,
+                     int levels, int cb, int nthreads, int32_t *status, const long *list, long n) {
+    return run(1, img, stream, X, Y, lut, lut_n, passes, levels, cb, nthreads, status, 0, 0, n, NULL, 0, list);
+}
+
+int bpco_decode_list(const int32_t *stream, int32_t *img, int X, int Y, const int *lut, int lut_n, int passes,
+                     int levels, int cb, int nthreads, int32_t *status, const long *list, long n) {
+    return run(0, stream, img, X, Y, lut, lut_n, passes, levels, cb, nthreads, status, 0, 0, n, NULL, 0, list);
 }
 
 /* LUT training counts of an image: adds, for every entry of the LUT layout
@@ -780,7 +803,7 @@ int bpco_lut_stats(const int32_t *img, int X, int Y, int passes, int levels, int
     }
     for (long q = 0; q < stats_n; q++) lut[q] = 64;
     int rc = run(1, img, scratch, X, Y, lut, (int)stats_n, passes, levels, cb, nthreads, NULL, 0, 0, -1, stats,
-                 stats_n);
+                 stats_n, NULL);
     free(lut);
     free(scratch);
     return rc < 0 ? rc : 0;

@@ -48,6 +48,11 @@ def lib():
                                   ctypes.c_int, ctypes.c_int, ctypes.c_int, i32p, ctypes.c_int, ctypes.c_long,
                                   ctypes.c_long]
         L.bpco_decode.restype = ctypes.c_int
+        lp = ctypes.POINTER(ctypes.c_long)
+        for f in (L.bpco_encode_list, L.bpco_decode_list):
+            f.argtypes = [i32p, i32p, ctypes.c_int, ctypes.c_int, i32p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                          ctypes.c_int, ctypes.c_int, i32p, lp, ctypes.c_long]
+            f.restype = ctypes.c_int
         L.bpco_find_subband.argtypes = [ctypes.c_int] * 5 + [ctypes.POINTER(ctypes.c_int)] * 2
         L.bpco_find_subband.restype = None
         L.bpco_block_msb.argtypes = [i32p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int]
@@ -106,6 +111,29 @@ def decode(stream: np.ndarray, shape, lut: np.ndarray, passes: int, levels: int 
     if rc < 0:
         raise ValueError(f"oracle decode: bad arguments ({rc})")
     return (out, st) if with_status else out
+
+
+def code_list(enc: bool, data: np.ndarray, shape, lut: np.ndarray, passes: int, levels: int, cb: int,
+              cb_list, out: np.ndarray | None = None, threads: int = 0):
+    """Encode (enc) or decode only the codeblocks in cb_list (raster indices)
+    of an X x Y image or slot stream.  `out` (X*Y int32, reused if given)
+    receives their slots / pixels; everything else in it is left untouched.
+    Returns (out, status per codeblock)."""
+    Y, X = shape
+    data = np.ascontiguousarray(data, dtype=np.int32).reshape(-1)
+    assert data.size == X * Y
+    lut = np.ascontiguousarray(lut, dtype=np.int32)
+    if out is None:
+        out = np.full(X * Y, -1 if enc else 0, np.int32)
+    assert out.dtype == np.int32 and out.size == X * Y and out.flags["C_CONTIGUOUS"]
+    lst = np.ascontiguousarray(cb_list, dtype=np.int64)
+    st = np.zeros((X // cb) * (Y // cb), np.int32)
+    f = lib().bpco_encode_list if enc else lib().bpco_decode_list
+    rc = f(_p(data), _p(out.reshape(-1)), X, Y, _p(lut), lut.size, passes, levels, cb, threads or os.cpu_count() or 1,
+           _p(st), lst.ctypes.data_as(ctypes.POINTER(ctypes.c_long)), lst.size)
+    if rc < 0:
+        raise ValueError(f"oracle {'encode' if enc else 'decode'} list: bad arguments ({rc})")
+    return out, st
 
 
 def find_subband(x: int, y: int, X: int, Y: int, levels: int):
