@@ -253,6 +253,8 @@ class Batch:
         L.bpc_batch_decode.argtypes = [vp, vp, vp, ctypes.POINTER(vp), vp, vp]
         L.bpc_batch_set_schedule.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int]
         L.bpc_batch_get_schedule.argtypes = [vp, ip, ip, ip, ip]
+        L.bpc_batch_set_tuning.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+        L.bpc_batch_get_tuning.argtypes = [vp, ip, ip, ip, ip]
         L.bpc_batch_tune.argtypes = [vp, ctypes.POINTER(vp), vp, vp, ctypes.POINTER(vp), vp,
                                      ctypes.POINTER(ctypes.c_double)]
         L.bpc_batch_destroy.argtypes = [vp]
@@ -295,6 +297,14 @@ class Batch:
         a, b, c, d = (ctypes.c_int() for _ in range(4))
         lib().bpc_batch_get_schedule(self.h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c), ctypes.byref(d))
         return a.value, b.value, c.value, bool(d.value)
+
+    def set_tuning(self, warps_enc: int = 4, warps_dec: int = 4, cost_enc: bool = False, cost_dec: bool = False):
+        _check(lib().bpc_batch_set_tuning(self.h, warps_enc, warps_dec, int(cost_enc), int(cost_dec)), "set_tuning")
+
+    def tuning(self):
+        a, b, c, d = (ctypes.c_int() for _ in range(4))
+        lib().bpc_batch_get_tuning(self.h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c), ctypes.byref(d))
+        return a.value, b.value, bool(c.value), bool(d.value)
 
     def tune(self, coeffs, compact, offsets, out) -> float:
         us = ctypes.c_double()

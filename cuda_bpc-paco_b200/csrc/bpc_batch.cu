@@ -23,6 +23,7 @@
 
 #include <algorithm>
 #include <cstdio>
+#include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_scan.cuh>
 #include <map>
 #include <vector>
@@ -91,10 +92,15 @@ __global__ void k_lut_bytes(const int *lut, int lut_n, uint8_t *tab, int tab_n, 
     }
 }
 
-template <int PASSES, int CBS, bool ENC>
-__global__ void __launch_bounds__(kWarps * 32, ENC ? kMinCtasEnc : kMinCtasDec)
-    k_bpc_batch(const BatchImage *imgs, const BatchItem *items, int nitems, unsigned *head, int *counts,
-                const long long *offsets, int *status) {
+// resident warps per SM the register budget is sized for, whatever the CTA shape
+constexpr int kResidentWarpsEnc = kMinCtasEnc * kWarps, kResidentWarpsDec = kMinCtasDec * kWarps;
+
+// WARPS warps per CTA (2, 4 or 8: a tuning choice); `order` (may be null)
+// lists the items in the order the queue hands them out
+template <int PASSES, int CBS, bool ENC, int WARPS>
+__global__ void __launch_bounds__(WARPS * 32, (ENC ? kResidentWarpsEnc : kResidentWarpsDec) / WARPS)
+    k_bpc_batch(const BatchImage *imgs, const BatchItem *items, const int *order, int nitems, unsigned *head,
+                int *counts, const long long *offsets, int *status) {
     using G = Geo<CBS>;
     extern __shared__ __align__(16) unsigned char smem[];
     const int warp = (int)(threadIdx.x >> 5);
@@ -113,7 +119,7 @@ __global__ void __launch_bounds__(kWarps * 32, ENC ? kMinCtasEnc : kMinCtasDec)
         if (w.lane() == 0) it = atomicAdd(head, 1u);
         it = w.shfl_idx(it, 0);
         if (it >= (unsigned)nitems) break;
-        const BatchItem item = items[it];
+        const BatchItem item = items[order ? order[it] : (int)it];
         const BatchImage im = imgs[item.image];
         Params p;
         p.in = im.in;
@@ -175,6 +181,64 @@ __global__ void k_gather(const BatchImage *imgs, int nimg, const long long *offs
     }
 }
 
+// Expected work of each work item, for the cost order of the queue (the
+// costs of the single-image work order, bpc_order.cu): decoder, per codeblock
+// the container words + 128 per bitplane decoded (MSB word); encoder, per
+// codeblock the bitplanes coded (MSB + 1, 33 for an all-zero codeblock) from
+// one read of its coefficients.  key = cost, val = item index.
+__global__ void k_item_cost_dec(const BatchItem *items, int nitems, const BatchImage *imgs,
+                                const long long *offsets, uint32_t *key, int *val) {
+    for (int it = (int)(blockIdx.x * blockDim.x + threadIdx.x); it < nitems; it += (int)(gridDim.x * blockDim.x)) {
+        const BatchItem item = items[it];
+        const BatchImage &im = imgs[item.image];
+        uint32_t cost = 0;
+        for (int k = 0; k < item.n; k++) {
+            const long long g = im.cb_base + item.cb0 + k;
+            const long long o0 = offsets[g], n = offsets[g + 1] - o0;
+            const int m = n > 0 && o0 >= 0 && o0 < im.in_words ? __ldg(im.in + o0) : -1;  // container base
+            const uint32_t planes = m == 32 ? 33u : (m >= 0 && m <= 27 ? (uint32_t)m + 1u : 0u);
+            cost += (uint32_t)(n < 0 ? 0 : (n > 4096 ? 4096 : n)) + 128u * planes;
+        }
+        key[it] = cost;
+        val[it] = it;
+    }
+}
+
+// one warp per item
+template <int CBS>
+__global__ void k_item_cost_enc(const BatchItem *items, int nitems, const BatchImage *imgs, uint32_t *key, int *val) {
+    using G = Geo<CBS>;
+    const int lane = (int)(threadIdx.x & 31u), grp = lane / G::NL, gl = lane % G::NL;
+    const int wstride = (int)(gridDim.x * blockDim.x) >> 5;
+    for (int it = (int)(blockIdx.x * blockDim.x + threadIdx.x) >> 5; it < nitems; it += wstride) {
+        const BatchItem item = items[it];
+        const BatchImage &im = imgs[item.image];
+        uint32_t cost = 0;
+        for (int k = 0; k < item.n; k += G::NG) {
+            const int cb = item.cb0 + k + grp;
+            uint32_t mx = 0;
+            const bool ok = k + grp < item.n;
+            if (ok) {
+                const int cbx = cb % im.ncbx, cby = cb / im.ncbx;
+                const int32_t *src = im.in + (size_t)cby * CBS * (size_t)im.X + (size_t)cbx * CBS + 2 * gl;
+                for (int i = 0; i < CBS; i++) {
+                    const int2 v = __ldg(reinterpret_cast<const int2 *>(src + (size_t)i * (size_t)im.X));
+                    mx |= (v.x < 0 ? 0u - (uint32_t)v.x : (uint32_t)v.x) |
+                          (v.y < 0 ? 0u - (uint32_t)v.y : (uint32_t)v.y);
+                }
+            }
+            for (int o = G::NL / 2; o; o >>= 1) mx |= __shfl_xor_sync(0xffffffffu, mx, o);
+            uint32_t c = ok ? (mx ? 32u - (uint32_t)__clz((int)mx) : 33u) : 0u;
+            if (G::NG == 2) c += __shfl_xor_sync(0xffffffffu, c, 16);
+            cost += c;
+        }
+        if (lane == 0) {
+            key[it] = cost;
+            val[it] = it;
+        }
+    }
+}
+
 }  // namespace bpc
 
 using namespace bpc;
@@ -220,6 +284,13 @@ struct Batch {
     int sms = 148;
     // schedule
     int ctas_enc = kMinCtasEnc, ctas_dec = kMinCtasDec, per_item = 4, use_graph = 1;
+    int warps_enc = kWarps, warps_dec = kWarps;  // warps per CTA: 2, 4 or 8
+    int cost_enc = 0, cost_dec = 0;              // queue order: 0 coarse subbands first, 1 cost order
+    // cost order buffers per class: keys and item indices, sorted copies
+    uint32_t *d_key[kClasses] = {}, *d_key_sorted[kClasses] = {};
+    int *d_val[kClasses] = {}, *d_order[kClasses] = {};
+    void *d_sort_tmp = nullptr;
+    size_t sort_tmp_bytes = 0;
     cudaStream_t side[kClasses - 1] = {};
     cudaEvent_t ev_fork = nullptr, ev_join[kClasses - 1] = {};
     Graph genc, gdec;
@@ -248,55 +319,115 @@ int build_items(Batch &b) {
             tmp[class_of(b.passes[i], cbs)].push_back({{i, k, std::min(step, ncb - k)}, lvl});
         }
     }
+    size_t sort_bytes = 0;
     for (int c = 0; c < kClasses; c++) {
         std::stable_sort(tmp[c].begin(), tmp[c].end(), [](const Tmp &a, const Tmp &z) { return a.weight > z.weight; });
         for (auto &t : tmp[c]) b.h_items[c].push_back(t.it);
         b.nitems[c] = (int)b.h_items[c].size();
         cudaFree(b.d_items[c]);
+        cudaFree(b.d_key[c]);
+        cudaFree(b.d_key_sorted[c]);
+        cudaFree(b.d_val[c]);
+        cudaFree(b.d_order[c]);
         b.d_items[c] = nullptr;
+        b.d_key[c] = b.d_key_sorted[c] = nullptr;
+        b.d_val[c] = b.d_order[c] = nullptr;
         if (b.nitems[c]) {
-            CUDA_TRY(cudaMalloc((void **)&b.d_items[c], b.nitems[c] * sizeof(BatchItem)));
-            CUDA_TRY(cudaMemcpy(b.d_items[c], b.h_items[c].data(), b.nitems[c] * sizeof(BatchItem),
-                                cudaMemcpyHostToDevice));
+            const size_t n = (size_t)b.nitems[c];
+            CUDA_TRY(cudaMalloc((void **)&b.d_items[c], n * sizeof(BatchItem)));
+            CUDA_TRY(cudaMemcpy(b.d_items[c], b.h_items[c].data(), n * sizeof(BatchItem), cudaMemcpyHostToDevice));
+            CUDA_TRY(cudaMalloc((void **)&b.d_key[c], n * sizeof(uint32_t)));
+            CUDA_TRY(cudaMalloc((void **)&b.d_key_sorted[c], n * sizeof(uint32_t)));
+            CUDA_TRY(cudaMalloc((void **)&b.d_val[c], n * sizeof(int)));
+            CUDA_TRY(cudaMalloc((void **)&b.d_order[c], n * sizeof(int)));
+            size_t t = 0;
+            CUDA_TRY(cub::DeviceRadixSort::SortPairsDescending(nullptr, t, b.d_key[c], b.d_key_sorted[c], b.d_val[c],
+                                                               b.d_order[c], b.nitems[c]));
+            sort_bytes = std::max(sort_bytes, t);
         }
+    }
+    if (sort_bytes > b.sort_tmp_bytes) {
+        cudaFree(b.d_sort_tmp);
+        b.d_sort_tmp = nullptr;
+        b.sort_tmp_bytes = 0;
+        CUDA_TRY(cudaMalloc(&b.d_sort_tmp, sort_bytes));
+        b.sort_tmp_bytes = sort_bytes;
     }
     return BPC_OK;
 }
 
-template <int PASSES, int CBS, bool ENC>
-cudaError_t launch_batch(const Batch &b, int cls, const BatchImage *imgs, const long long *offsets, int *status,
-                         cudaStream_t st) {
+template <int PASSES, int CBS, bool ENC, int WARPS>
+cudaError_t launch_batch_w(const Batch &b, int cls, const BatchImage *imgs, const int *order,
+                           const long long *offsets, int *status, cudaStream_t st) {
     using G = Geo<CBS>;
-    const size_t sm = (size_t)kSignTableBytes + (size_t)kWarps * 4u * (size_t)(ENC ? 512 : G::RING_WORDS);
-    cudaError_t e = cudaFuncSetAttribute(k_bpc_batch<PASSES, CBS, ENC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)sm);
+    const size_t sm = (size_t)kSignTableBytes + (size_t)WARPS * 4u * (size_t)(ENC ? 512 : G::RING_WORDS);
+    cudaError_t e = cudaFuncSetAttribute(k_bpc_batch<PASSES, CBS, ENC, WARPS>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return e;
     const int grid = std::max(1, std::min(b.sms * (ENC ? b.ctas_enc : b.ctas_dec),
-                                          (b.nitems[cls] + kWarps - 1) / kWarps));
-    k_bpc_batch<PASSES, CBS, ENC><<<grid, kWarps * 32, sm, st>>>(imgs, b.d_items[cls], b.nitems[cls], b.d_head + cls,
-                                                                 ENC ? b.d_counts : nullptr, offsets, status);
+                                          (b.nitems[cls] + WARPS - 1) / WARPS));
+    k_bpc_batch<PASSES, CBS, ENC, WARPS><<<grid, WARPS * 32, sm, st>>>(
+        imgs, b.d_items[cls], order, b.nitems[cls], b.d_head + cls, ENC ? b.d_counts : nullptr, offsets, status);
     return cudaGetLastError();
 }
 
-cudaError_t launch_class(const Batch &b, int cls, bool enc, const BatchImage *imgs, const long long *offsets,
-                         int *status, cudaStream_t st) {
+template <int PASSES, int CBS, bool ENC>
+cudaError_t launch_batch(const Batch &b, int cls, const BatchImage *imgs, const int *order,
+                         const long long *offsets, int *status, cudaStream_t st) {
+    switch (ENC ? b.warps_enc : b.warps_dec) {
+        case 2: return launch_batch_w<PASSES, CBS, ENC, 2>(b, cls, imgs, order, offsets, status, st);
+        case 8: return launch_batch_w<PASSES, CBS, ENC, 8>(b, cls, imgs, order, offsets, status, st);
+        default: return launch_batch_w<PASSES, CBS, ENC, 4>(b, cls, imgs, order, offsets, status, st);
+    }
+}
+
+cudaError_t launch_class(const Batch &b, int cls, bool enc, const BatchImage *imgs, const int *order,
+                         const long long *offsets, int *status, cudaStream_t st) {
     if (b.nitems[cls] == 0) return cudaSuccess;
     switch (cls) {
-        case 0: return enc ? launch_batch<2, 64, true>(b, cls, imgs, offsets, status, st)
-                           : launch_batch<2, 64, false>(b, cls, imgs, offsets, status, st);
-        case 1: return enc ? launch_batch<2, 32, true>(b, cls, imgs, offsets, status, st)
-                           : launch_batch<2, 32, false>(b, cls, imgs, offsets, status, st);
-        case 2: return enc ? launch_batch<3, 64, true>(b, cls, imgs, offsets, status, st)
-                           : launch_batch<3, 64, false>(b, cls, imgs, offsets, status, st);
-        default: return enc ? launch_batch<3, 32, true>(b, cls, imgs, offsets, status, st)
-                            : launch_batch<3, 32, false>(b, cls, imgs, offsets, status, st);
+        case 0: return enc ? launch_batch<2, 64, true>(b, cls, imgs, order, offsets, status, st)
+                           : launch_batch<2, 64, false>(b, cls, imgs, order, offsets, status, st);
+        case 1: return enc ? launch_batch<2, 32, true>(b, cls, imgs, order, offsets, status, st)
+                           : launch_batch<2, 32, false>(b, cls, imgs, order, offsets, status, st);
+        case 2: return enc ? launch_batch<3, 64, true>(b, cls, imgs, order, offsets, status, st)
+                           : launch_batch<3, 64, false>(b, cls, imgs, order, offsets, status, st);
+        default: return enc ? launch_batch<3, 32, true>(b, cls, imgs, order, offsets, status, st)
+                            : launch_batch<3, 32, false>(b, cls, imgs, order, offsets, status, st);
     }
+}
+
+// cost order of one class's queue on stream s: item costs, then the item
+// indices sorted by cost, descending
+cudaError_t order_class(const Batch &b, int cls, bool enc, const BatchImage *imgs, const long long *offsets,
+                        cudaStream_t s) {
+    const int n = b.nitems[cls];
+    if (enc) {
+        const int grid = std::min((n + 7) / 8, 4096);
+        if (cls == 1 || cls == 3)
+            k_item_cost_enc<32><<<grid, 256, 0, s>>>(b.d_items[cls], n, imgs, b.d_key[cls], b.d_val[cls]);
+        else
+            k_item_cost_enc<64><<<grid, 256, 0, s>>>(b.d_items[cls], n, imgs, b.d_key[cls], b.d_val[cls]);
+    } else {
+        const int grid = std::min((n + 255) / 256, 1024);
+        k_item_cost_dec<<<grid, 256, 0, s>>>(b.d_items[cls], n, imgs, offsets, b.d_key[cls], b.d_val[cls]);
+    }
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    size_t tmp = b.sort_tmp_bytes;
+    return cub::DeviceRadixSort::SortPairsDescending(b.d_sort_tmp, tmp, b.d_key[cls], b.d_key_sorted[cls],
+                                                     b.d_val[cls], b.d_order[cls], n, 0, 32, s);
 }
 
 // enqueue one whole encode or decode on `st` (forks the classes onto side streams)
 int enqueue(Batch &b, bool enc, const BatchImage *imgs, int32_t *compact, const long long *offsets_in,
             long long *offsets_out, int *status, cudaStream_t st) {
     CUDA_TRY(cudaMemsetAsync(b.d_head, 0, kClasses * sizeof(unsigned), st));
+    // cost order: every class's queue sorted first (they share the sort
+    // workspace), then the class kernels fork
+    const bool cost = enc ? b.cost_enc : b.cost_dec;
+    if (cost)
+        for (int c = 0; c < kClasses; c++)
+            if (b.nitems[c]) CUDA_TRY(order_class(b, c, enc, imgs, enc ? nullptr : offsets_in, st));
     CUDA_TRY(cudaEventRecord(b.ev_fork, st));
     int used = 0;
     for (int c = 0; c < kClasses; c++) {
@@ -306,7 +437,7 @@ int enqueue(Batch &b, bool enc, const BatchImage *imgs, int32_t *compact, const 
             s = b.side[used - 1];
             CUDA_TRY(cudaStreamWaitEvent(s, b.ev_fork, 0));
         }
-        CUDA_TRY(launch_class(b, c, enc, imgs, enc ? nullptr : offsets_in, status, s));
+        CUDA_TRY(launch_class(b, c, enc, imgs, cost ? b.d_order[c] : nullptr, enc ? nullptr : offsets_in, status, s));
         if (used > 0) CUDA_TRY(cudaEventRecord(b.ev_join[used - 1], s));
         used++;
     }
@@ -408,6 +539,13 @@ void free_batch(Batch *b) {
         if (b->ev_join[k]) cudaEventDestroy(b->ev_join[k]);
     }
     if (b->ev_fork) cudaEventDestroy(b->ev_fork);
+    for (int c = 0; c < kClasses; c++) {
+        cudaFree(b->d_key[c]);
+        cudaFree(b->d_key_sorted[c]);
+        cudaFree(b->d_val[c]);
+        cudaFree(b->d_order[c]);
+    }
+    cudaFree(b->d_sort_tmp);
     if (b->genc.exec) cudaGraphExecDestroy(b->genc.exec);
     if (b->gdec.exec) cudaGraphExecDestroy(b->gdec.exec);
     delete b;
@@ -501,8 +639,9 @@ long long bpc_batch_words(const void *batch) { return batch ? ((const Batch *)ba
 
 int bpc_batch_set_schedule(void *batch, int ctas_per_sm_enc, int ctas_per_sm_dec, int cbs_per_item, int use_graph) {
     Batch *b = (Batch *)batch;
-    if (!b || ctas_per_sm_enc < 1 || ctas_per_sm_enc > kMinCtasEnc || ctas_per_sm_dec < 1 ||
-        ctas_per_sm_dec > kMinCtasDec || cbs_per_item < 1 || cbs_per_item > 64)
+    // CTAs per SM up to the resident warps the kernels are built for
+    if (!b || ctas_per_sm_enc < 1 || ctas_per_sm_enc * b->warps_enc > kResidentWarpsEnc || ctas_per_sm_dec < 1 ||
+        ctas_per_sm_dec * b->warps_dec > kResidentWarpsDec || cbs_per_item < 1 || cbs_per_item > 64)
         return BPC_ERR_ARG;
     b->ctas_enc = ctas_per_sm_enc;
     b->ctas_dec = ctas_per_sm_dec;
@@ -515,6 +654,34 @@ int bpc_batch_set_schedule(void *batch, int ctas_per_sm_enc, int ctas_per_sm_dec
     if (b->genc.exec) cudaGraphExecDestroy(b->genc.exec);
     if (b->gdec.exec) cudaGraphExecDestroy(b->gdec.exec);
     b->genc.exec = b->gdec.exec = nullptr;
+    return BPC_OK;
+}
+
+int bpc_batch_set_tuning(void *batch, int warps_per_cta_enc, int warps_per_cta_dec, int cost_order_enc,
+                         int cost_order_dec) {
+    Batch *b = (Batch *)batch;
+    auto ok_w = [](int w) { return w == 2 || w == 4 || w == 8; };
+    if (!b || !ok_w(warps_per_cta_enc) || !ok_w(warps_per_cta_dec)) return BPC_ERR_ARG;
+    b->warps_enc = warps_per_cta_enc;
+    b->warps_dec = warps_per_cta_dec;
+    b->cost_enc = cost_order_enc ? 1 : 0;
+    b->cost_dec = cost_order_dec ? 1 : 0;
+    b->ctas_enc = std::min(b->ctas_enc, kResidentWarpsEnc / b->warps_enc);
+    b->ctas_dec = std::min(b->ctas_dec, kResidentWarpsDec / b->warps_dec);
+    if (b->genc.exec) cudaGraphExecDestroy(b->genc.exec);
+    if (b->gdec.exec) cudaGraphExecDestroy(b->gdec.exec);
+    b->genc.exec = b->gdec.exec = nullptr;
+    return BPC_OK;
+}
+
+int bpc_batch_get_tuning(const void *batch, int *warps_per_cta_enc, int *warps_per_cta_dec, int *cost_order_enc,
+                         int *cost_order_dec) {
+    const Batch *b = (const Batch *)batch;
+    if (!b) return BPC_ERR_ARG;
+    if (warps_per_cta_enc) *warps_per_cta_enc = b->warps_enc;
+    if (warps_per_cta_dec) *warps_per_cta_dec = b->warps_dec;
+    if (cost_order_enc) *cost_order_enc = b->cost_enc;
+    if (cost_order_dec) *cost_order_dec = b->cost_dec;
     return BPC_OK;
 }
 
@@ -559,8 +726,10 @@ int bpc_batch_decode(void *batch, const int *d_compact, const long long *d_offse
 }
 
 // Autotuner: time encode and decode under each schedule on the caller's
-// buffers and keep the fastest (codeblocks per work item shared by both
-// directions, CTAs per SM per direction).  Returns the best total in us.
+// buffers and keep the fastest: codeblocks per work item (shared by both
+// directions) and CTAs per SM per direction, then per direction the warps per
+// CTA (2, 4, 8 at the same resident warps) and the queue order.  Returns the
+// best total in us.
 int bpc_batch_tune(void *batch, const int *const *d_coeffs, int *d_compact, long long *d_offsets, int *const *d_out,
                    void *stream, double *best_us) {
     Batch *b = (Batch *)batch;
@@ -571,6 +740,9 @@ int bpc_batch_tune(void *batch, const int *const *d_coeffs, int *d_compact, long
     CUDA_TRY(cudaEventCreate(&e1));
     const int items[] = {1, 2, 4, 8};
     double best = 1e30;
+    // first CTAs per SM and codeblocks per item with 4-warp CTAs and the
+    // coarse-subbands-first queue
+    if (const int rc0 = bpc_batch_set_tuning(batch, kWarps, kWarps, 0, 0)) return rc0;
     int bi = b->per_item, be = b->ctas_enc, bd = b->ctas_dec;
     auto timed = [&](bool enc, float &ms) -> int {
         float acc = 0.f;
@@ -607,10 +779,40 @@ int bpc_batch_tune(void *batch, const int *const *d_coeffs, int *d_compact, long
         }
         if (te_best + td_best < best) best = te_best + td_best, bi = it, be = ce, bd = cd;
     }
+    int rc = bpc_batch_set_schedule(batch, be, bd, bi, b->use_graph);
+    if (rc) return rc;
+    // then, per direction, the CTA shape at the same resident warps per SM
+    // and the queue order (coarse subbands first, or sorted by cost)
+    for (int dir = 0; dir < 2; dir++) {
+        const bool enc = dir == 0;
+        const int wpsm = (enc ? be : bd) * kWarps;
+        float t_best = 1e30f;
+        int w_best = kWarps, o_best = 0;
+        for (int wc : {2, 4, 8})
+            for (int ord = 0; ord < 2; ord++) {
+                const int ce = enc ? std::max(1, wpsm / wc) : b->ctas_enc, cd = enc ? b->ctas_dec : std::max(1, wpsm / wc);
+                if ((rc = bpc_batch_set_tuning(batch, enc ? wc : b->warps_enc, enc ? b->warps_dec : wc,
+                                               enc ? ord : b->cost_enc, enc ? b->cost_dec : ord)))
+                    return rc;
+                if ((rc = bpc_batch_set_schedule(batch, ce, cd, bi, b->use_graph))) return rc;
+                float t;
+                if ((rc = timed(enc, t))) return rc;
+                if (t < t_best) t_best = t, w_best = wc, o_best = ord;
+            }
+        if ((rc = bpc_batch_set_tuning(batch, enc ? w_best : b->warps_enc, enc ? b->warps_dec : w_best,
+                                       enc ? o_best : b->cost_enc, enc ? b->cost_dec : o_best)))
+            return rc;
+        const int ce = enc ? std::max(1, wpsm / w_best) : b->ctas_enc, cd = enc ? b->ctas_dec : std::max(1, wpsm / w_best);
+        if ((rc = bpc_batch_set_schedule(batch, ce, cd, bi, b->use_graph))) return rc;
+        if (enc)
+            best = t_best;
+        else
+            best += t_best;
+    }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     if (best_us) *best_us = best * 1e3;
-    return bpc_batch_set_schedule(batch, be, bd, bi, b->use_graph);
+    return BPC_OK;
 }
 
 int bpc_batch_destroy(void *batch) {

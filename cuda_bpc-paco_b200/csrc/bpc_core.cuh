@@ -334,7 +334,8 @@ struct Coder {
     int32_t *slot_out;
     uint32_t in_cap;  // decoder: words readable at slot_in (slot size, or the compact length)
     int lane, gl, g, msb;
-    int top;  // highest stored bitplane (-1: none)
+    int top;        // highest bitplane coded from the stored planes (-1: none)
+    uint32_t qtop;  // encoder: per quarter q, byte q = 1 + the highest plane stored for it (0: none)
     uint32_t gmask, ltmask;
     uint64_t B[2];  // encoder: magnitude bits of the current plane; decoder: decoded 1-bits
     int sig_base, sign_base;  // LUT byte indices of the current plane and pass
@@ -425,9 +426,14 @@ struct Coder {
     BPC_FI void plane_begin(int b) {
         if (ENC) {
             if (b <= top) {
+                // a quarter's planes above its own highest set bit were never
+                // stored: they read as zero
                 const uint32_t *q = planes[b];
-                B[0] = (uint64_t)q[0] | ((uint64_t)q[1] << 32);
-                B[1] = (uint64_t)q[2] | ((uint64_t)q[3] << 32);
+                const uint32_t u = (uint32_t)b;
+                const uint32_t q0 = u < (qtop & 0xFFu) ? q[0] : 0u, q1 = u < ((qtop >> 8) & 0xFFu) ? q[1] : 0u;
+                const uint32_t q2 = u < ((qtop >> 16) & 0xFFu) ? q[2] : 0u, q3 = u < (qtop >> 24) ? q[3] : 0u;
+                B[0] = (uint64_t)q0 | ((uint64_t)q1 << 32);
+                B[1] = (uint64_t)q2 | ((uint64_t)q3 << 32);
             } else {
                 B[0] = B[1] = 0ull;
             }
@@ -1006,17 +1012,41 @@ struct Coder {
         top = -1;
         if (ENC) {
             slot_out = p.out + (ok ? (size_t)cb * cap : 0);
-            // Read_Coefficients :14-44 + Find_MSB :114-161: signs and OR
+            // Read_Coefficients :14-44 + Find_MSB :114-161 in one read: per
+            // 32-row half, one 8-byte load per row gives the lane's two
+            // columns; signs go to N, magnitudes through a 32x32 bit
+            // transpose to bitplanes 0..27 (those up to the quarter's own
+            // highest set bit are stored)
             uint32_t mx = 0;
+            qtop = 0u;
             if (ok) {
-                for (int i = 0; i < CBS; i++) {
-                    int32_t v0, v1;
-                    w.load2(src + (size_t)i * (size_t)p.X, v0, v1);
-                    const uint32_t m0 = v0 < 0 ? 0u - (uint32_t)v0 : (uint32_t)v0;
-                    const uint32_t m1 = v1 < 0 ? 0u - (uint32_t)v1 : (uint32_t)v1;
-                    s.N[0] |= (uint64_t)(v0 < 0) << i;
-                    s.N[1] |= (uint64_t)(v1 < 0) << i;
-                    mx |= m0 | m1;
+#pragma unroll 1
+                for (int h = 0; h < NH; h++) {
+                    uint32_t a0[32], a1[32], o0 = 0, o1 = 0, n0 = 0, n1 = 0;
+#pragma unroll
+                    for (int r = 0; r < 32; r++) {
+                        int32_t v0, v1;
+                        w.load2(src + (size_t)(h * 32 + r) * (size_t)p.X, v0, v1);
+                        a0[r] = v0 < 0 ? 0u - (uint32_t)v0 : (uint32_t)v0;
+                        a1[r] = v1 < 0 ? 0u - (uint32_t)v1 : (uint32_t)v1;
+                        n0 |= (uint32_t)(v0 < 0) << r;
+                        n1 |= (uint32_t)(v1 < 0) << r;
+                        o0 |= a0[r];
+                        o1 |= a1[r];
+                    }
+                    s.N[0] |= (uint64_t)n0 << (32 * h);
+                    s.N[1] |= (uint64_t)n1 << (32 * h);
+                    mx |= o0 | o1;
+                    const int t0 = o0 ? 31 - clz32(o0) : -1, t1 = o1 ? 31 - clz32(o1) : -1;
+                    qtop |= (uint32_t)(t0 + 1) << (8 * h) | (uint32_t)(t1 + 1) << (8 * (2 + h));
+                    transpose32(a0);
+#pragma unroll
+                    for (int k = 0; k < 28; k++)
+                        if (k <= t0) planes[k][h] = a0[k];
+                    transpose32(a1);
+#pragma unroll
+                    for (int k = 0; k < 28; k++)
+                        if (k <= t1) planes[k][2 + h] = a1[k];
                 }
             }
             if (mx >= (1u << 28)) s.status |= ST_INPUT_RANGE;
@@ -1024,24 +1054,7 @@ struct Coder {
             if (ok) {
                 msb = mx ? 31 - clz32(mx) : 32;
                 if (gl == 0 && !STATS) slot_out[0] = msb;  // :1155
-                // bitplanes 0..min(MSB, 27): transpose 32 rows x 32 bits at a time
-                top = msb <= 27 ? msb : -1;
-                if (top >= 0) {
-#pragma unroll 1
-                    for (int q = 0; q < 2 * NH; q++) {
-                        const int c = q / NH, h = q % NH;
-                        uint32_t a[32];
-#pragma unroll
-                        for (int r = 0; r < 32; r++) {
-                            const int32_t v = w.load1(src + (size_t)(h * 32 + r) * (size_t)p.X + c);
-                            a[r] = v < 0 ? 0u - (uint32_t)v : (uint32_t)v;
-                        }
-                        transpose32(a);
-#pragma unroll
-                        for (int k = 0; k < 28; k++)
-                            if (k <= top) planes[k][c * 2 + h] = a[k];
-                    }
-                }
+                top = msb <= 27 ? msb : -1;  // planes >= 28 are flag bits, not magnitudes
             }
             // neighbour sign columns are data: lane-1's right, lane+1's left
             const uint64_t up = shfl_up64(w, s.N[1]), dn = shfl_down64(w, s.N[0]);
