@@ -404,13 +404,20 @@ def run_batched(args):
             lut_dev[(ps, lv)] = bpc.DeviceLut(luts[ps], ps, lv)
     slot = torch.empty(8192 * 8192, dtype=torch.int32, device="cuda")
 
-    def plain_step(times=None):
+    def plain_step(times=None, spans=None):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         for k, (X, Y, lv, ps, cb) in enumerate(specs):
             sv = slot[:X * Y]
+            if spans is not None:
+                a = torch.cuda.Event(enable_timing=True)
+                a.record(stream)
             bpc.encode_device(d_in[k], sv, lut_dev[(ps, lv)], cb)
             bpc.decode_device(sv, out[k], lut_dev[(ps, lv)], cb)
+            if spans is not None:
+                z = torch.cuda.Event(enable_timing=True)
+                z.record(stream)
+                spans.append((a, z))
         e1.record(stream)
         if times is not None:
             times.append((e0, e1))
@@ -422,6 +429,13 @@ def run_batched(args):
         plain_step(pt)
     torch.cuda.synchronize()
     tp = sum(a.elapsed_time(b_) for a, b_ in pt) / len(pt) / 1e3
+    # GPU busy and idle time of one plain step: the per-image encode+decode
+    # spans against the whole step (the gaps are launch and host overhead)
+    spans, one = [], []
+    plain_step(one, spans)
+    torch.cuda.synchronize()
+    plain_busy = sum(a.elapsed_time(z) for a, z in spans) / 1e3
+    plain_total = one[0][0].elapsed_time(one[0][1]) / 1e3
     value = 2 * total / (te + td) / 1e9
     peak, peak_kind = load_peaks()
     words = int(offs_h[-1])
@@ -437,6 +451,8 @@ def run_batched(args):
                                 "graph": sched[3], "tuned_us_24_images": tuned_us}},
         "encode_gcoeffs": total / te / 1e9, "decode_gcoeffs": total / td / 1e9,
         "plain_per_image_gcoeffs": 2 * total / tp / 1e9, "batched_over_plain": tp / (te + td),
+        "plain_step_ms": 1e3 * plain_total, "plain_gpu_busy_ms": 1e3 * plain_busy,
+        "plain_gpu_idle_ms_per_image": 1e3 * (plain_total - plain_busy) / len(specs),
         "compact_words": words, "compression": 4.0 * total / (4.0 * words),
         "status": status, "images_lossless": lossless, "codeblocks_checked_vs_plain_stream": checked,
         "gpu_launches": "4 persistent kernels + scan + gather per encode, 4 per decode (one CUDA graph each)",
