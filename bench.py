@@ -85,6 +85,17 @@ def ncu_import(path, workload):
         i = col[m]
         return float(r[i].replace(",", "")) * scale.get(units[i], 1)
 
+    def dram(r, which):
+        """bytes read or written; from the throughput metric when the sum is absent"""
+        if f"dram__bytes_{which}.sum" in col:
+            return val(r, f"dram__bytes_{which}.sum")
+        if which == "read" and "dram__bytes.sum.per_second" in col:  # read + write together
+            i = col["dram__bytes.sum.per_second"]
+            rate = {"byte/s": 1, "Kbyte/s": 1e3, "Mbyte/s": 1e6, "Gbyte/s": 1e9, "Tbyte/s": 1e12}
+            per_s = float(r[i].replace(",", "")) * rate.get(units[i].replace("second", "s"), 1)
+            return per_s * val(r, "gpu__time_duration.sum") * 1e-6
+        return 0.0
+
     acc = {}
     for r in rows[hdr + 2:]:
         if len(r) != len(names) or "k_bpc" not in r[col["Kernel Name"]] or "batch" in r[col["Kernel Name"]]:
@@ -94,8 +105,8 @@ def ncu_import(path, workload):
         a = acc.setdefault(kind, [0, 0.0, 0.0, 0.0, 0.0])
         a[0] += 1
         a[1] += val(r, "gpu__time_duration.sum")
-        a[2] += val(r, "dram__bytes_read.sum")
-        a[3] += val(r, "dram__bytes_write.sum")
+        a[2] += dram(r, "read")
+        a[3] += dram(r, "write")
         a[4] += val(r, "smsp__inst_executed.sum")
     for kind, (n, t, rd, wr, ins) in sorted(acc.items()):
         print(f"{workload} {kind} {n} {t / n:.1f} {rd / n:.0f} {wr / n:.0f} {ins / n:.0f}")
