@@ -355,8 +355,10 @@ def run_batched(args):
     so = torch.zeros(sub.codeblocks + 1, dtype=torch.int64, device="cuda")
     tuned_us = sub.tune(d_in[:24], sc, so, out[:24])
     sched = sub.schedule()
+    tuning = sub.tuning()
     sub.close()
     del sc, so
+    b.set_tuning(*tuning)
     b.set_schedule(*sched)
     stream = torch.cuda.current_stream()
 
@@ -459,7 +461,9 @@ def run_batched(args):
         "config": {"workload": f"cfg3 batch: {len(specs)} images, {total / 1e9:.2f} G coefficients, sides 2048-8192, "
                                f"levels 3-6, 64x64 (70%) / 32x32, 2/3 passes", "l2": "inputs >> L2",
                    "schedule": {"ctas_per_sm_enc": sched[0], "ctas_per_sm_dec": sched[1], "cbs_per_item": sched[2],
-                                "graph": sched[3], "tuned_us_24_images": tuned_us}},
+                                "graph": sched[3], "warps_per_cta_enc": tuning[0], "warps_per_cta_dec": tuning[1],
+                                "cost_order_enc": tuning[2], "cost_order_dec": tuning[3],
+                                "tuned_us_24_images": tuned_us}},
         "encode_gcoeffs": total / te / 1e9, "decode_gcoeffs": total / td / 1e9,
         "plain_per_image_gcoeffs": 2 * total / tp / 1e9, "batched_over_plain": tp / (te + td),
         "plain_step_ms": 1e3 * plain_total, "plain_gpu_busy_ms": 1e3 * plain_busy,
