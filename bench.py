@@ -695,7 +695,7 @@ def run_ours(args, c):
         # the sampler polls every 50 ms: keep the GPU busy for a moment
         # before the timed region so that samples under load exist
         t_pre = time.perf_counter()
-        while time.perf_counter() - t_pre < 0.3:
+        while time.perf_counter() - t_pre < 0.3 and not (args.no_e2e or args.chain_only):  # profiling runs skip it
             step()
             torch.cuda.synchronize()
         torch.cuda.synchronize()
@@ -711,6 +711,24 @@ def run_ours(args, c):
     t_step = (te + td) / args.steps
     t_step = max_over_ranks(t_step, dev)
     value = 2 * N * world / t_step / 1e9
+
+    # the serial chain: the top codeblock row coded alone as an X x cb image
+    # (its codeblocks keep their subbands, since the subband of a codeblock of
+    # the top row depends on x only); its LL codeblocks are the longest
+    # lockstep chains of the whole image
+    top = cb * X
+    chain = {}
+    probes = (("encode_ms", lambda: bpc.encode_device(d_img[:cb], d_stream[:top], lut, cb, d_status)),
+              ("decode_ms", lambda: bpc.decode_device(d_stream[:top], d_dec[:cb], lut, cb, d_status)))
+    if (cb >> levels) >= 1:  # else the top row's subbands would depend on y
+        for name, fn in probes:
+            chain[name] = 1e3 * _timed(fn, stream, flush, 10, 3)
+    chain["what"] = f"top codeblock row alone ({X}x{cb}, {X // cb} codeblocks)" if chain else "n/a"
+    if args.chain_only:
+        if rank == 0:
+            print(json.dumps({"chain": chain}))
+        lut.close()
+        return
 
     if args.no_e2e:
         lut.close()
@@ -773,7 +791,7 @@ def run_ours(args, c):
         "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded generator + 5/3 DWT)",
         "config": bench_config(args, c, world),
         "encode_gcoeffs": N / te1 / 1e9, "decode_gcoeffs": N / td1 / 1e9,
-        "encode_ms": 1e3 * te1, "decode_ms": 1e3 * td1,
+        "encode_ms": 1e3 * te1, "decode_ms": 1e3 * td1, "chain": chain,
         "e2e": {"value": e2e, "unit": "Gcoeff/s", "h2d_bytes_per_step": 2 * 4 * N, "d2h_bytes_per_step": 2 * 4 * N + 8,
                 "ms_per_step": 1e3 * e2e_step, "copy_floor_ms": 1e3 * floor, "frac_of_floor": floor / e2e_step,
                 "copy_floor": "pinned H2D + D2H of X*Y int32 each, both directions at once, per call, x2 calls"},
@@ -934,6 +952,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="kernel timing only (profiling runs)")
     ap.add_argument("--no-ref-kernel", action="store_true", help="skip timing the rebuilt reference kernel")
+    ap.add_argument("--chain-only", action="store_true", help="stop after timing the top codeblock row alone")
     ap.add_argument("--ncu-import", help="print counter lines for profiles/k_bpc_counters.txt from ncu raw csv")
     ap.add_argument("--workload", default="cfg2", help="--ncu-import: workload name of the capture")
     args = ap.parse_args()
