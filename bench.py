@@ -349,15 +349,19 @@ def run_batched(args):
     offs = torch.zeros(b.codeblocks + 1, dtype=torch.int64, device="cuda")
     out = [torch.empty_like(t) for t in d_in]
     st = torch.zeros(1, dtype=torch.int32, device="cuda")
-    # autotune on a 24-image sub-batch, apply to the whole batch
-    sub = bpc.Batch(specs[:24], luts)
-    sc = torch.empty(sub.words, dtype=torch.int32, device="cuda")
-    so = torch.zeros(sub.codeblocks + 1, dtype=torch.int64, device="cuda")
-    tuned_us = sub.tune(d_in[:24], sc, so, out[:24])
-    sched = sub.schedule()
-    tuning = sub.tuning()
-    sub.close()
-    del sc, so
+    # autotune on a 24-image sub-batch, apply to the whole batch (--no-tune:
+    # the default schedule, e.g. for profiling runs)
+    if args.no_tune:
+        tuned_us, sched, tuning = None, b.schedule(), b.tuning()
+    else:
+        sub = bpc.Batch(specs[:24], luts)
+        sc = torch.empty(sub.words, dtype=torch.int32, device="cuda")
+        so = torch.zeros(sub.codeblocks + 1, dtype=torch.int64, device="cuda")
+        tuned_us = sub.tune(d_in[:24], sc, so, out[:24])
+        sched = sub.schedule()
+        tuning = sub.tuning()
+        sub.close()
+        del sc, so
     b.set_tuning(*tuning)
     b.set_schedule(*sched)
     stream = torch.cuda.current_stream()
@@ -953,6 +957,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="kernel timing only (profiling runs)")
     ap.add_argument("--no-ref-kernel", action="store_true", help="skip timing the rebuilt reference kernel")
     ap.add_argument("--chain-only", action="store_true", help="stop after timing the top codeblock row alone")
+    ap.add_argument("--no-tune", action="store_true", help="cfg3: keep the default batch schedule")
     ap.add_argument("--ncu-import", help="print counter lines for profiles/k_bpc_counters.txt from ncu raw csv")
     ap.add_argument("--workload", default="cfg2", help="--ncu-import: workload name of the capture")
     args = ap.parse_args()
