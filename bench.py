@@ -467,6 +467,7 @@ def run_batched(args):
                    "schedule": {"ctas_per_sm_enc": sched[0], "ctas_per_sm_dec": sched[1], "cbs_per_item": sched[2],
                                 "graph": sched[3], "warps_per_cta_enc": tuning[0], "warps_per_cta_dec": tuning[1],
                                 "cost_order_enc": tuning[2], "cost_order_dec": tuning[3],
+                                "classes_in_sequence_enc": tuning[4], "classes_in_sequence_dec": tuning[5],
                                 "tuned_us_24_images": tuned_us}},
         "encode_gcoeffs": total / te / 1e9, "decode_gcoeffs": total / td / 1e9,
         "plain_per_image_gcoeffs": 2 * total / tp / 1e9, "batched_over_plain": tp / (te + td),

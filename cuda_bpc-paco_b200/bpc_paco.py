@@ -253,8 +253,8 @@ class Batch:
         L.bpc_batch_decode.argtypes = [vp, vp, vp, ctypes.POINTER(vp), vp, vp]
         L.bpc_batch_set_schedule.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int]
         L.bpc_batch_get_schedule.argtypes = [vp, ip, ip, ip, ip]
-        L.bpc_batch_set_tuning.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int]
-        L.bpc_batch_get_tuning.argtypes = [vp, ip, ip, ip, ip]
+        L.bpc_batch_set_tuning.argtypes = [vp] + [ctypes.c_int] * 6
+        L.bpc_batch_get_tuning.argtypes = [vp] + [ip] * 6
         L.bpc_batch_tune.argtypes = [vp, ctypes.POINTER(vp), vp, vp, ctypes.POINTER(vp), vp,
                                      ctypes.POINTER(ctypes.c_double)]
         L.bpc_batch_destroy.argtypes = [vp]
@@ -298,13 +298,15 @@ class Batch:
         lib().bpc_batch_get_schedule(self.h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c), ctypes.byref(d))
         return a.value, b.value, c.value, bool(d.value)
 
-    def set_tuning(self, warps_enc: int = 4, warps_dec: int = 4, cost_enc: bool = False, cost_dec: bool = False):
-        _check(lib().bpc_batch_set_tuning(self.h, warps_enc, warps_dec, int(cost_enc), int(cost_dec)), "set_tuning")
+    def set_tuning(self, warps_enc: int = 4, warps_dec: int = 4, cost_enc: bool = False, cost_dec: bool = False,
+                   seq_enc: bool = False, seq_dec: bool = False):
+        _check(lib().bpc_batch_set_tuning(self.h, warps_enc, warps_dec, int(cost_enc), int(cost_dec), int(seq_enc),
+                                          int(seq_dec)), "set_tuning")
 
     def tuning(self):
-        a, b, c, d = (ctypes.c_int() for _ in range(4))
-        lib().bpc_batch_get_tuning(self.h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c), ctypes.byref(d))
-        return a.value, b.value, bool(c.value), bool(d.value)
+        v = [ctypes.c_int() for _ in range(6)]
+        lib().bpc_batch_get_tuning(self.h, *[ctypes.byref(x) for x in v])
+        return v[0].value, v[1].value, bool(v[2].value), bool(v[3].value), bool(v[4].value), bool(v[5].value)
 
     def tune(self, coeffs, compact, offsets, out) -> float:
         us = ctypes.c_double()

@@ -286,6 +286,7 @@ struct Batch {
     int ctas_enc = kMinCtasEnc, ctas_dec = kMinCtasDec, per_item = 4, use_graph = 1;
     int warps_enc = kWarps, warps_dec = kWarps;  // warps per CTA: 2, 4 or 8
     int cost_enc = 0, cost_dec = 0;              // queue order: 0 coarse subbands first, 1 cost order
+    int seq_enc = 0, seq_dec = 0;                // class kernels: 0 concurrent (forked streams), 1 one after another
     // cost order buffers per class: keys and item indices, sorted copies
     uint32_t *d_key[kClasses] = {}, *d_key_sorted[kClasses] = {};
     int *d_val[kClasses] = {}, *d_order[kClasses] = {};
@@ -429,10 +430,17 @@ int enqueue(Batch &b, bool enc, const BatchImage *imgs, int32_t *compact, const 
         for (int c = 0; c < kClasses; c++)
             if (b.nitems[c]) CUDA_TRY(order_class(b, c, enc, imgs, enc ? nullptr : offsets_in, st));
     CUDA_TRY(cudaEventRecord(b.ev_fork, st));
+    // one after another: each class kernel has the GPU (and its instruction
+    // caches) to itself, at the price of one tail per class
+    const bool seq = enc ? b.seq_enc : b.seq_dec;
     int used = 0;
     for (int c = 0; c < kClasses; c++) {
         if (!b.nitems[c]) continue;
         cudaStream_t s = st;
+        if (seq) {
+            CUDA_TRY(launch_class(b, c, enc, imgs, cost ? b.d_order[c] : nullptr, enc ? nullptr : offsets_in, status, st));
+            continue;
+        }
         if (used > 0) {
             s = b.side[used - 1];
             CUDA_TRY(cudaStreamWaitEvent(s, b.ev_fork, 0));
@@ -658,7 +666,7 @@ int bpc_batch_set_schedule(void *batch, int ctas_per_sm_enc, int ctas_per_sm_dec
 }
 
 int bpc_batch_set_tuning(void *batch, int warps_per_cta_enc, int warps_per_cta_dec, int cost_order_enc,
-                         int cost_order_dec) {
+                         int cost_order_dec, int classes_in_sequence_enc, int classes_in_sequence_dec) {
     Batch *b = (Batch *)batch;
     auto ok_w = [](int w) { return w == 2 || w == 4 || w == 8; };
     if (!b || !ok_w(warps_per_cta_enc) || !ok_w(warps_per_cta_dec)) return BPC_ERR_ARG;
@@ -666,6 +674,8 @@ int bpc_batch_set_tuning(void *batch, int warps_per_cta_enc, int warps_per_cta_d
     b->warps_dec = warps_per_cta_dec;
     b->cost_enc = cost_order_enc ? 1 : 0;
     b->cost_dec = cost_order_dec ? 1 : 0;
+    b->seq_enc = classes_in_sequence_enc ? 1 : 0;
+    b->seq_dec = classes_in_sequence_dec ? 1 : 0;
     b->ctas_enc = std::min(b->ctas_enc, kResidentWarpsEnc / b->warps_enc);
     b->ctas_dec = std::min(b->ctas_dec, kResidentWarpsDec / b->warps_dec);
     if (b->genc.exec) cudaGraphExecDestroy(b->genc.exec);
@@ -675,13 +685,15 @@ int bpc_batch_set_tuning(void *batch, int warps_per_cta_enc, int warps_per_cta_d
 }
 
 int bpc_batch_get_tuning(const void *batch, int *warps_per_cta_enc, int *warps_per_cta_dec, int *cost_order_enc,
-                         int *cost_order_dec) {
+                         int *cost_order_dec, int *classes_in_sequence_enc, int *classes_in_sequence_dec) {
     const Batch *b = (const Batch *)batch;
     if (!b) return BPC_ERR_ARG;
     if (warps_per_cta_enc) *warps_per_cta_enc = b->warps_enc;
     if (warps_per_cta_dec) *warps_per_cta_dec = b->warps_dec;
     if (cost_order_enc) *cost_order_enc = b->cost_enc;
     if (cost_order_dec) *cost_order_dec = b->cost_dec;
+    if (classes_in_sequence_enc) *classes_in_sequence_enc = b->seq_enc;
+    if (classes_in_sequence_dec) *classes_in_sequence_dec = b->seq_dec;
     return BPC_OK;
 }
 
@@ -742,7 +754,7 @@ int bpc_batch_tune(void *batch, const int *const *d_coeffs, int *d_compact, long
     double best = 1e30;
     // first CTAs per SM and codeblocks per item with 4-warp CTAs and the
     // coarse-subbands-first queue
-    if (const int rc0 = bpc_batch_set_tuning(batch, kWarps, kWarps, 0, 0)) return rc0;
+    if (const int rc0 = bpc_batch_set_tuning(batch, kWarps, kWarps, 0, 0, 0, 0)) return rc0;
     int bi = b->per_item, be = b->ctas_enc, bd = b->ctas_dec;
     auto timed = [&](bool enc, float &ms) -> int {
         float acc = 0.f;
@@ -781,27 +793,31 @@ int bpc_batch_tune(void *batch, const int *const *d_coeffs, int *d_compact, long
     }
     int rc = bpc_batch_set_schedule(batch, be, bd, bi, b->use_graph);
     if (rc) return rc;
-    // then, per direction, the CTA shape at the same resident warps per SM
-    // and the queue order (coarse subbands first, or sorted by cost)
+    // then, per direction, the CTA shape at the same resident warps per SM,
+    // the queue order (coarse subbands first, or sorted by cost) and whether
+    // the class kernels run concurrently or one after another
     for (int dir = 0; dir < 2; dir++) {
         const bool enc = dir == 0;
         const int wpsm = (enc ? be : bd) * kWarps;
         float t_best = 1e30f;
-        int w_best = kWarps, o_best = 0;
+        int w_best = kWarps, o_best = 0, q_best = 0;
+        auto apply = [&](int wc, int ord, int sq) {
+            return bpc_batch_set_tuning(batch, enc ? wc : b->warps_enc, enc ? b->warps_dec : wc,
+                                        enc ? ord : b->cost_enc, enc ? b->cost_dec : ord, enc ? sq : b->seq_enc,
+                                        enc ? b->seq_dec : sq);
+        };
         for (int wc : {2, 4, 8})
-            for (int ord = 0; ord < 2; ord++) {
-                const int ce = enc ? std::max(1, wpsm / wc) : b->ctas_enc, cd = enc ? b->ctas_dec : std::max(1, wpsm / wc);
-                if ((rc = bpc_batch_set_tuning(batch, enc ? wc : b->warps_enc, enc ? b->warps_dec : wc,
-                                               enc ? ord : b->cost_enc, enc ? b->cost_dec : ord)))
-                    return rc;
-                if ((rc = bpc_batch_set_schedule(batch, ce, cd, bi, b->use_graph))) return rc;
-                float t;
-                if ((rc = timed(enc, t))) return rc;
-                if (t < t_best) t_best = t, w_best = wc, o_best = ord;
-            }
-        if ((rc = bpc_batch_set_tuning(batch, enc ? w_best : b->warps_enc, enc ? b->warps_dec : w_best,
-                                       enc ? o_best : b->cost_enc, enc ? b->cost_dec : o_best)))
-            return rc;
+            for (int ord = 0; ord < 2; ord++)
+                for (int sq = 0; sq < 2; sq++) {
+                    const int ce = enc ? std::max(1, wpsm / wc) : b->ctas_enc;
+                    const int cd = enc ? b->ctas_dec : std::max(1, wpsm / wc);
+                    if ((rc = apply(wc, ord, sq))) return rc;
+                    if ((rc = bpc_batch_set_schedule(batch, ce, cd, bi, b->use_graph))) return rc;
+                    float t;
+                    if ((rc = timed(enc, t))) return rc;
+                    if (t < t_best) t_best = t, w_best = wc, o_best = ord, q_best = sq;
+                }
+        if ((rc = apply(w_best, o_best, q_best))) return rc;
         const int ce = enc ? std::max(1, wpsm / w_best) : b->ctas_enc, cd = enc ? b->ctas_dec : std::max(1, wpsm / w_best);
         if ((rc = bpc_batch_set_schedule(batch, ce, cd, bi, b->use_graph))) return rc;
         if (enc)

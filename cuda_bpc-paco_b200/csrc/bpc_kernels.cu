@@ -46,8 +46,11 @@ struct GpuWarp {
     __device__ __forceinline__ void atomic_or(int *p, int v) { atomicOr(p, v); }
 };
 
-template <int PASSES, int CBS, bool ENC>
-__global__ void __launch_bounds__(kWarps * 32, ENC ? kMinCtasEnc : kMinCtasDec) k_bpc(Params p) {
+// WARPS codeblock warps per CTA: kWarps, or 1 for decodes of at most half a wave
+// (their heaviest codeblocks then land on different SMs, see launch_t); the
+// register budget stays that of kMinCtas x kWarps resident warps per SM
+template <int PASSES, int CBS, bool ENC, int WARPS = kWarps>
+__global__ void __launch_bounds__(WARPS * 32, (ENC ? kMinCtasEnc : kMinCtasDec) * kWarps / WARPS) k_bpc(Params p) {
     using G = Geo<CBS>;
     extern __shared__ __align__(16) unsigned char smem[];
     uint8_t *tab = smem;
@@ -72,8 +75,8 @@ __global__ void __launch_bounds__(kWarps * 32, ENC ? kMinCtasEnc : kMinCtasDec) 
     uint32_t planes[28][4];  // per-thread bitplanes (local memory, L1-resident)
     uint8_t ev_key[ENC ? kEvKeys : 1];
     uint32_t ev_val[ENC ? kEvVals : 1];
-    const int stride = (int)gridDim.x * kWarps * G::NG;
-    for (int base = p.cb_begin + ((int)blockIdx.x * kWarps + warp) * G::NG; base < p.cb_end; base += stride) {
+    const int stride = (int)gridDim.x * WARPS * G::NG;
+    for (int base = p.cb_begin + ((int)blockIdx.x * WARPS + warp) * G::NG; base < p.cb_end; base += stride) {
         Coder<PASSES, CBS, ENC, GpuWarp> cd(w, p, ring, tab, sgtab, planes, ev_key, ev_val);
         cd.run(p.order ? p.order[base / G::NG] : base);
     }
@@ -114,24 +117,37 @@ cudaError_t launch_stats(int passes, int cbs, const Params &p, unsigned long lon
     return cbs == 64 ? launch_stats_t<3, 64>(p, stats, st) : launch_stats_t<3, 32>(p, stats, st);
 }
 
-template <int PASSES, int CBS, bool ENC>
+template <int PASSES, int CBS, bool ENC, int WARPS>
 static size_t smem_bytes(const Params &p) {
     using G = Geo<CBS>;
-    return (size_t)p.tab_n + (size_t)kSignTableBytes + (size_t)kWarps * 4u * (size_t)(ENC ? 512 : G::RING_WORDS);
+    return (size_t)p.tab_n + (size_t)kSignTableBytes + (size_t)WARPS * 4u * (size_t)(ENC ? 512 : G::RING_WORDS);
+}
+
+template <int PASSES, int CBS, bool ENC, int WARPS>
+static cudaError_t launch_w(const Params &p, int grid, int warps_needed, cudaStream_t st) {
+    const size_t sm = smem_bytes<PASSES, CBS, ENC, WARPS>(p);
+    cudaError_t e =
+        cudaFuncSetAttribute(k_bpc<PASSES, CBS, ENC, WARPS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return e;
+    const int full = (warps_needed + WARPS - 1) / WARPS;
+    if (grid <= 0 || grid > full) grid = full;
+    if (grid < 1) grid = 1;
+    k_bpc<PASSES, CBS, ENC, WARPS><<<grid, WARPS * 32, sm, st>>>(p);
+    return cudaGetLastError();
 }
 
 template <int PASSES, int CBS, bool ENC>
 static cudaError_t launch_t(const Params &p, int grid, cudaStream_t st) {
     using G = Geo<CBS>;
-    const size_t sm = smem_bytes<PASSES, CBS, ENC>(p);
-    cudaError_t e = cudaFuncSetAttribute(k_bpc<PASSES, CBS, ENC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    if (e != cudaSuccess) return e;
     const int warps_needed = (p.cb_end - p.cb_begin + G::NG - 1) / G::NG;
-    const int full = (warps_needed + kWarps - 1) / kWarps;
-    if (grid <= 0 || grid > full) grid = full;
-    if (grid < 1) grid = 1;
-    k_bpc<PASSES, CBS, ENC><<<grid, kWarps * 32, sm, st>>>(p);
-    return cudaGetLastError();
+    // A decode of at most half a wave of resident warps runs one warp per CTA:
+    // consecutive CTAs go to different SMs, so its heaviest codeblocks (the
+    // coarse subbands, neighbours in raster order) do not share an SM's
+    // instruction cache and shared-memory pipes (a 2048x2048 decode: 0.375 ->
+    // 0.358 ms).  Fuller decodes keep 4-warp CTAs, which measured faster there.
+    if (!ENC && grid <= 0 && 2LL * warps_needed <= (long long)resident_warps(false, -1))
+        return launch_w<PASSES, CBS, ENC, 1>(p, grid, warps_needed, st);
+    return launch_w<PASSES, CBS, ENC, kWarps>(p, grid, warps_needed, st);
 }
 
 cudaError_t launch_code(bool enc, int passes, int cbs, const Params &p, int grid, cudaStream_t st) {

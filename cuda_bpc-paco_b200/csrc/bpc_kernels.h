@@ -39,6 +39,8 @@ cudaError_t launch_code(bool enc, int passes, int cbs, const Params &p, int grid
 // the image's work units by expected cost and set *order to the order to put
 // in Params; *order stays null (raster order) for images of at most two waves.
 long long sched_ints(int ncb, int cbs);
+// warps of the plain coder resident at once on device `dev` (-1: current)
+int resident_warps(bool enc, int dev);
 // more than two waves on device `dev` (-1: the current device)
 bool order_pays(bool enc, int ncb, int cbs, int dev = -1);
 cudaError_t plan_order(bool enc, int cbs, const Params &p, int *sched, cudaStream_t st, const int **order);

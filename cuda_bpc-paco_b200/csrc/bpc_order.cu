@@ -138,6 +138,8 @@ __global__ void __launch_bounds__(kBuckets) k_order(const uint32_t *key, int uni
     }
 }
 
+}  // namespace
+
 // warps resident at once on device `dev` (-1: the current device; SM count
 // cached per device; callers may be on any host thread)
 int resident_warps(bool enc, int dev) {
@@ -151,6 +153,8 @@ int resident_warps(bool enc, int dev) {
     }
     return n * kWarps * (enc ? kMinCtasEnc : kMinCtasDec);
 }
+
+namespace {
 
 template <int CBS>
 cudaError_t plan_t(bool enc, const Params &p, int *sched, cudaStream_t st, const int **order) {

@@ -167,18 +167,20 @@ int bpc_batch_decode(void *batch, const int *d_compact, const long long *d_offse
 int bpc_batch_set_schedule(void *batch, int ctas_per_sm_enc, int ctas_per_sm_dec, int cbs_per_item, int use_graph);
 int bpc_batch_get_schedule(const void *batch, int *ctas_per_sm_enc, int *ctas_per_sm_dec, int *cbs_per_item,
                            int *use_graph);
-/* Further schedule dimensions: warps per CTA of the persistent kernels (2, 4
- * or 8; CTAs per SM times warps per CTA may not exceed 16 for the encoder and
- * 28 for the decoder, and bpc_batch_set_tuning lowers the CTAs per SM to fit)
- * and the order in which the device queue hands out work items: 0 = coarse
- * subbands first (fixed at creation), 1 = sorted by expected cost on the GPU
- * before every call (decoder: container words + 128 per bitplane, from the
- * offsets and MSB words; encoder: bitplanes, from one extra read of the
- * coefficients).  Outputs never depend on any schedule setting. */
+/* Further schedule dimensions, per direction: warps per CTA of the persistent
+ * kernels (2, 4 or 8; CTAs per SM times warps per CTA may not exceed 16 for the
+ * encoder and 28 for the decoder, and bpc_batch_set_tuning lowers the CTAs per
+ * SM to fit); the order in which the device queue hands out work items (0 =
+ * coarse subbands first, fixed at creation; 1 = sorted by expected cost on the
+ * GPU before every call: decoder container words + 128 per bitplane from the
+ * offsets and MSB words, encoder bitplanes from one extra read of the
+ * coefficients); and whether the kernels of the (passes, codeblock size)
+ * classes run concurrently on forked streams (0) or one after another (1).
+ * Outputs never depend on any schedule setting. */
 int bpc_batch_set_tuning(void *batch, int warps_per_cta_enc, int warps_per_cta_dec, int cost_order_enc,
-                         int cost_order_dec);
+                         int cost_order_dec, int classes_in_sequence_enc, int classes_in_sequence_dec);
 int bpc_batch_get_tuning(const void *batch, int *warps_per_cta_enc, int *warps_per_cta_dec, int *cost_order_enc,
-                         int *cost_order_dec);
+                         int *cost_order_dec, int *classes_in_sequence_enc, int *classes_in_sequence_dec);
 int bpc_batch_tune(void *batch, const int *const *d_coeffs, int *d_compact, long long *d_offsets, int *const *d_out,
                    void *stream, double *best_us);
 int bpc_batch_destroy(void *batch);

@@ -61,14 +61,14 @@ def run_batch(b, d_in, torch):
 
 @pytest.mark.parametrize("schedule,tuning", [
     (None, None), ((4, 7, 1, True), None), ((2, 3, 4, False), None), ((1, 2, 8, True), None),
-    ((8, 14, 2, True), (2, 2, True, True)), ((2, 3, 4, True), (8, 8, True, False)),
-    ((2, 3, 1, False), (4, 8, False, True))])
+    ((8, 14, 2, True), (2, 2, True, True, False, True)), ((2, 3, 4, True), (8, 8, True, False, True, False)),
+    ((2, 3, 1, False), (4, 8, False, True, True, True))])
 def test_batch_matches_oracle(batch_setup, schedule, tuning):
     """Every schedule (CTAs per SM, codeblocks per item, graph; warps per CTA
     and cost-ordered queues) gives the same container and decode."""
     import torch
     b, imgs, d_in, (want_words, want_dec, want_st) = batch_setup
-    b.set_tuning(*(tuning or (4, 4, False, False)))
+    b.set_tuning(*(tuning or (4, 4, False, False, False, False)))
     if schedule:
         b.set_schedule(*schedule)
     for _ in range(2):  # second call replays the captured graph
@@ -93,7 +93,7 @@ def test_batch_tune(batch_setup):
     us = b.tune(d_in, compact, offs, out)
     assert us > 0
     ce, cd, per, graph = b.schedule()
-    we, wd, _, _ = b.tuning()
+    we, wd, _, _, _, _ = b.tuning()
     assert we in (2, 4, 8) and wd in (2, 4, 8)
     assert 1 <= ce * we <= 16 and 1 <= cd * wd <= 28 and per in (1, 2, 4, 8)
     compact, offs, out, st = run_batch(b, d_in, torch)
