@@ -81,30 +81,6 @@ int fill_params(bpc::Params &p, bool enc, const int *in, int *out, int X, int Y,
     return BPC_OK;
 }
 
-int code_device(bool enc, const int *in, int *out, int X, int Y, const int *d_lut, int lut_n, int passes, int levels,
-                int cb, int *d_status, int *d_counts, int grid, void *stream, int cb_begin = 0, int cb_end = -1,
-                int *sched = nullptr) {
-    bpc::Params p;
-    const int rc = fill_params(p, enc, in, out, X, Y, d_lut, lut_n, passes, levels, cb, d_status, d_counts);
-    if (rc) return rc;
-    if (cb_end >= 0) {
-        p.cb_begin = cb_begin;
-        p.cb_end = cb_end;
-    }
-    if (sched && grid <= 0) {
-        const cudaError_t e = bpc::plan_order(enc, cb, p, sched, (cudaStream_t)stream, &p.order);
-        if (e != cudaSuccess) {
-            std::fprintf(stderr, "bpc: work-order launch failed: %s\n", cudaGetErrorString(e));
-            return BPC_ERR_CUDA;
-        }
-    }
-    const cudaError_t e = bpc::launch_code(enc, passes, cb, p, grid, (cudaStream_t)stream);
-    if (e != cudaSuccess) {
-        std::fprintf(stderr, "bpc: kernel launch failed: %s\n", cudaGetErrorString(e));
-        return BPC_ERR_CUDA;
-    }
-    return BPC_OK;
-}
 
 #define CUDA_TRY(x)                                                                              \
     do {                                                                                         \
@@ -185,7 +161,7 @@ int code_host_locked(DropInState &s, int direction, int *hdata, int X, int Y, co
         cudaStream_t st = s.streams[k % nst];
         const size_t off = (size_t)r0 * row_words, cnt = (size_t)(r1 - r0) * row_words;
         CUDA_TRY(cudaMemcpyAsync(s.d_a + off, hdata + off, cnt * sizeof(int), cudaMemcpyHostToDevice, st));
-        const int rc = code_device(direction == BPC_CODE, s.d_a, s.d_b, X, Y, d_lut, lut_n, passes, levels, cb,
+        const int rc = bpc::code_device(direction == BPC_CODE, s.d_a, s.d_b, X, Y, d_lut, lut_n, passes, levels, cb,
                                    s.d_status, nullptr, 0, st, r0 * ncbx, r1 * ncbx);
         if (rc) return rc;
         CUDA_TRY(cudaMemcpyAsync(hdata + off, s.d_b + off, cnt * sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -201,6 +177,35 @@ int code_host_locked(DropInState &s, int direction, int *hdata, int X, int Y, co
 }
 
 }  // namespace
+
+namespace bpc {
+
+int code_device(bool enc, const int *in, int *out, int X, int Y, const int *d_lut, int lut_n, int passes, int levels,
+                int cb, int *d_status, int *d_counts, int grid, void *stream, int cb_begin, int cb_end, int *sched,
+                bool latency_forms) {
+    Params p;
+    const int rc = fill_params(p, enc, in, out, X, Y, d_lut, lut_n, passes, levels, cb, d_status, d_counts);
+    if (rc) return rc;
+    if (cb_end >= 0) {
+        p.cb_begin = cb_begin;
+        p.cb_end = cb_end;
+    }
+    if (sched && grid <= 0) {
+        const cudaError_t e = plan_order(enc, cb, p, sched, (cudaStream_t)stream, &p.order);
+        if (e != cudaSuccess) {
+            std::fprintf(stderr, "bpc: work-order launch failed: %s\n", cudaGetErrorString(e));
+            return BPC_ERR_CUDA;
+        }
+    }
+    const cudaError_t e = launch_code(enc, passes, cb, p, grid, (cudaStream_t)stream, latency_forms);
+    if (e != cudaSuccess) {
+        std::fprintf(stderr, "bpc: kernel launch failed: %s\n", cudaGetErrorString(e));
+        return BPC_ERR_CUDA;
+    }
+    return BPC_OK;
+}
+
+}  // namespace bpc
 
 extern "C" {
 
@@ -346,13 +351,13 @@ int bpc_code_host(int direction, int *hdata, int X, int Y, const int *d_lut, int
 
 int bpc_encode_device(const int *d_coeffs, int *d_stream, int X, int Y, const int *d_lut, int lut_n, int passes,
                       int levels, int cb_size, int *d_status, int *d_counts, int grid, void *stream) {
-    return code_device(true, d_coeffs, d_stream, X, Y, d_lut, lut_n, passes, levels, cb_size, d_status, d_counts, grid,
+    return bpc::code_device(true, d_coeffs, d_stream, X, Y, d_lut, lut_n, passes, levels, cb_size, d_status, d_counts, grid,
                        stream);
 }
 
 int bpc_decode_device(const int *d_stream, int *d_coeffs, int X, int Y, const int *d_lut, int lut_n, int passes,
                       int levels, int cb_size, int *d_status, int *d_counts, int grid, void *stream) {
-    return code_device(false, d_stream, d_coeffs, X, Y, d_lut, lut_n, passes, levels, cb_size, d_status, d_counts,
+    return bpc::code_device(false, d_stream, d_coeffs, X, Y, d_lut, lut_n, passes, levels, cb_size, d_status, d_counts,
                        grid, stream);
 }
 
@@ -364,14 +369,14 @@ long long bpc_sched_ints(int X, int Y, int cb_size) {
 int bpc_encode_device_sched(const int *d_coeffs, int *d_stream, int X, int Y, const int *d_lut, int lut_n, int passes,
                             int levels, int cb_size, int *d_status, int *d_counts, int *d_sched, void *stream) {
     if (!d_sched) return BPC_ERR_ARG;
-    return code_device(true, d_coeffs, d_stream, X, Y, d_lut, lut_n, passes, levels, cb_size, d_status, d_counts, 0,
+    return bpc::code_device(true, d_coeffs, d_stream, X, Y, d_lut, lut_n, passes, levels, cb_size, d_status, d_counts, 0,
                        stream, 0, -1, d_sched);
 }
 
 int bpc_decode_device_sched(const int *d_stream, int *d_coeffs, int X, int Y, const int *d_lut, int lut_n, int passes,
                             int levels, int cb_size, int *d_status, int *d_counts, int *d_sched, void *stream) {
     if (!d_sched) return BPC_ERR_ARG;
-    return code_device(false, d_stream, d_coeffs, X, Y, d_lut, lut_n, passes, levels, cb_size, d_status, d_counts, 0,
+    return bpc::code_device(false, d_stream, d_coeffs, X, Y, d_lut, lut_n, passes, levels, cb_size, d_status, d_counts, 0,
                        stream, 0, -1, d_sched);
 }
 

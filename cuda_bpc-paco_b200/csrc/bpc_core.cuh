@@ -320,7 +320,13 @@ BPC_FI uint64_t shfl_down64(W &w, uint64_t v) {
     return ((uint64_t)hi << 32) | lo;
 }
 
-template <int PASSES, int CBS, bool ENC, class W>
+// LAT selects the latency form of the per-lane loops, for launches whose time is
+// the serial chain of their heaviest codeblocks rather than the SMs' issue rate:
+// the encoder codes two positions per loop iteration (two independent
+// extractions and table reads ahead of the two sequential coder updates), the
+// decoder reads a step's sign context before its significance decision.  Both
+// execute more instructions per symbol; the bitstream is the same.
+template <int PASSES, int CBS, bool ENC, class W, bool LAT = false>
 struct Coder {
     using G = Geo<CBS>;
     static constexpr int NH = CBS / 32;  // 32-row halves per column
@@ -470,6 +476,20 @@ struct Coder {
         const uint32_t wl = win3h<H>(Lm, j), wm = win3h<H>(Sc, j), wr = win3h<H>(Rm, j);
         const uint32_t nbh = wl | ((wm & 5u) << 3) | (wr << 6);
         const uint64_t bit = maskh<H>(1u, j), bit0 = c ? 0ull : bit, bit1 = c ? bit : 0ull;
+        // sign context of this coefficient (Compute_Sign_Context :178-226 over
+        // l, r, u, b): one lookup in the sign-context table indexed by the
+        // neighbours' bits, all decided before this step.  The latency form
+        // reads it (and its probability) now, off the decision's chain.
+        const uint64_t LN = c ? s.N[0] : s.XNL, MN = c ? s.N[1] : s.N[0], RN = c ? s.XNR : s.N[1];
+        uint32_t se = 0, P2e = 0;
+        auto sign_ctx = [&]() {
+            const uint32_t nl = bith<H>(LN, j), nr = bith<H>(RN, j), wmn = win3h<H>(MN, j);
+            const uint32_t sk = ((wl >> 1) & 1u) | (nl << 1) | ((wr & 2u) << 1) | (nr << 3) | ((wm & 1u) << 4) |
+                                ((wmn & 1u) << 5) | ((wm & 4u) << 4) | ((wmn & 4u) << 5);
+            se = sgtab[sk];
+            P2e = tab[sign_base + (int)(se & 3u)];
+        };
+        if (LAT) sign_ctx();
         bool coded = cand;
         if (PK == PK_SPP && PASSES == 3) {
             if (cand && nbh == 0) {  // SPP defers to CP (:450-452)
@@ -497,15 +517,10 @@ struct Coder {
             B[1] |= bit1;
         }
         if (!w.any(ns)) return;
-        // sign call (Compute_Sign_Context :178-226 over l, r, u, b): one lookup
-        // in the sign-context table indexed by the neighbours' bits
-        const uint64_t LN = c ? s.N[0] : s.XNL, MN = c ? s.N[1] : s.N[0], RN = c ? s.XNR : s.N[1];
-        const uint32_t nl = bith<H>(LN, j), nr = bith<H>(RN, j), wmn = win3h<H>(MN, j);
-        const uint32_t sk = ((wl >> 1) & 1u) | (nl << 1) | ((wr & 2u) << 1) | (nr << 3) | ((wm & 1u) << 4) |
-                            ((wmn & 1u) << 5) | ((wm & 4u) << 4) | ((wmn & 4u) << 5);
-        const uint32_t se = sgtab[sk];
-        const uint32_t sidx = se & 3u, pred = se >> 2;
-        const uint32_t P2 = ns ? tab[sign_base + (int)sidx] : 0u;
+        // sign call
+        if (!LAT) sign_ctx();
+        const uint32_t pred = se >> 2;
+        const uint32_t P2 = ns ? P2e : 0u;
         const uint32_t neg = (ac_dec(ns, P2) ^ pred) & 1u;
         if (ns && neg) {
             s.N[0] |= bit0;
@@ -879,21 +894,49 @@ struct Coder {
                 s1 = zip16(si[0][1], si[1][1], q);
                 gq = zip16(sg[0], sg[1], q);
             }
-            do {
-                const int t = ctz32(kq);
-                kq &= kq - 1;
-                const int key = (32 * q + t) * 2;  // (row, column, phase) in the pass
-                if (PK == PK_MRP) {
-                    enc_symbol_if(true, (yq >> t) & 1u, Pref, key);
-                } else {
-                    const uint32_t ctx = ((c0 >> t) & 1u) | (((c1 >> t) & 1u) << 1) | (((c2 >> t) & 1u) << 2) |
-                                         (((c3 >> t) & 1u) << 3);
-                    enc_symbol_if(true, (yq >> t) & 1u, tab[sig_b + (int)ctx], key);
-                    // the sign call of a coefficient that became significant
-                    const uint32_t sidx = ((s0 >> t) & 1u) | (((s1 >> t) & 1u) << 1);
-                    enc_symbol_if(((nq >> t) & 1u) != 0u, (gq >> t) & 1u, tab[sign_b + (int)sidx], key + 1);
-                }
-            } while (kq);
+            if constexpr (LAT) {  // two positions per iteration, the second predicated
+                do {
+                    const int t = ctz32(kq);
+                    kq &= kq - 1;
+                    const bool two = kq != 0u;
+                    const int t2 = two ? ctz32(kq) : t;
+                    kq &= two ? kq - 1 : kq;
+                    const int key = (32 * q + t) * 2, key2 = (32 * q + t2) * 2;
+                    if (PK == PK_MRP) {
+                        enc_symbol_if(true, (yq >> t) & 1u, Pref, key);
+                        enc_symbol_if(two, (yq >> t2) & 1u, Pref, key2);
+                    } else {
+                        const uint32_t ca = ((c0 >> t) & 1u) | (((c1 >> t) & 1u) << 1) | (((c2 >> t) & 1u) << 2) |
+                                            (((c3 >> t) & 1u) << 3);
+                        const uint32_t cb2 = ((c0 >> t2) & 1u) | (((c1 >> t2) & 1u) << 1) | (((c2 >> t2) & 1u) << 2) |
+                                             (((c3 >> t2) & 1u) << 3);
+                        const uint32_t sa = ((s0 >> t) & 1u) | (((s1 >> t) & 1u) << 1);
+                        const uint32_t sb = ((s0 >> t2) & 1u) | (((s1 >> t2) & 1u) << 1);
+                        const uint32_t Pa = tab[sig_b + (int)ca], P2a = tab[sign_b + (int)sa];
+                        const uint32_t Pb = tab[sig_b + (int)cb2], P2b = tab[sign_b + (int)sb];
+                        enc_symbol_if(true, (yq >> t) & 1u, Pa, key);
+                        enc_symbol_if(((nq >> t) & 1u) != 0u, (gq >> t) & 1u, P2a, key + 1);
+                        enc_symbol_if(two, (yq >> t2) & 1u, Pb, key2);
+                        enc_symbol_if(two && ((nq >> t2) & 1u) != 0u, (gq >> t2) & 1u, P2b, key2 + 1);
+                    }
+                } while (kq);
+            } else {
+                do {
+                    const int t = ctz32(kq);
+                    kq &= kq - 1;
+                    const int key = (32 * q + t) * 2;  // (row, column, phase) in the pass
+                    if (PK == PK_MRP) {
+                        enc_symbol_if(true, (yq >> t) & 1u, Pref, key);
+                    } else {
+                        const uint32_t ctx = ((c0 >> t) & 1u) | (((c1 >> t) & 1u) << 1) |
+                                             (((c2 >> t) & 1u) << 2) | (((c3 >> t) & 1u) << 3);
+                        enc_symbol_if(true, (yq >> t) & 1u, tab[sig_b + (int)ctx], key);
+                        // the sign call of a coefficient that became significant
+                        const uint32_t sidx = ((s0 >> t) & 1u) | (((s1 >> t) & 1u) << 1);
+                        enc_symbol_if(((nq >> t) & 1u) != 0u, (gq >> t) & 1u, tab[sign_b + (int)sidx], key + 1);
+                    }
+                } while (kq);
+            }
         }
         enc_rank();
     }

@@ -49,7 +49,7 @@ struct GpuWarp {
 // WARPS codeblock warps per CTA: kWarps, or 1 for decodes of at most half a wave
 // (their heaviest codeblocks then land on different SMs, see launch_t); the
 // register budget stays that of kMinCtas x kWarps resident warps per SM
-template <int PASSES, int CBS, bool ENC, int WARPS = kWarps>
+template <int PASSES, int CBS, bool ENC, int WARPS = kWarps, bool LAT = false>
 __global__ void __launch_bounds__(WARPS * 32, (ENC ? kMinCtasEnc : kMinCtasDec) * kWarps / WARPS) k_bpc(Params p) {
     using G = Geo<CBS>;
     extern __shared__ __align__(16) unsigned char smem[];
@@ -77,7 +77,7 @@ __global__ void __launch_bounds__(WARPS * 32, (ENC ? kMinCtasEnc : kMinCtasDec) 
     uint32_t ev_val[ENC ? kEvVals : 1];
     const int stride = (int)gridDim.x * WARPS * G::NG;
     for (int base = p.cb_begin + ((int)blockIdx.x * WARPS + warp) * G::NG; base < p.cb_end; base += stride) {
-        Coder<PASSES, CBS, ENC, GpuWarp> cd(w, p, ring, tab, sgtab, planes, ev_key, ev_val);
+        Coder<PASSES, CBS, ENC, GpuWarp, LAT> cd(w, p, ring, tab, sgtab, planes, ev_key, ev_val);
         cd.run(p.order ? p.order[base / G::NG] : base);
     }
 }
@@ -123,41 +123,56 @@ static size_t smem_bytes(const Params &p) {
     return (size_t)p.tab_n + (size_t)kSignTableBytes + (size_t)WARPS * 4u * (size_t)(ENC ? 512 : G::RING_WORDS);
 }
 
-template <int PASSES, int CBS, bool ENC, int WARPS>
+template <int PASSES, int CBS, bool ENC, int WARPS, bool LAT>
 static cudaError_t launch_w(const Params &p, int grid, int warps_needed, cudaStream_t st) {
     const size_t sm = smem_bytes<PASSES, CBS, ENC, WARPS>(p);
-    cudaError_t e =
-        cudaFuncSetAttribute(k_bpc<PASSES, CBS, ENC, WARPS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    cudaError_t e = cudaFuncSetAttribute(k_bpc<PASSES, CBS, ENC, WARPS, LAT>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return e;
     const int full = (warps_needed + WARPS - 1) / WARPS;
     if (grid <= 0 || grid > full) grid = full;
     if (grid < 1) grid = 1;
-    k_bpc<PASSES, CBS, ENC, WARPS><<<grid, WARPS * 32, sm, st>>>(p);
+    k_bpc<PASSES, CBS, ENC, WARPS, LAT><<<grid, WARPS * 32, sm, st>>>(p);
     return cudaGetLastError();
 }
 
 template <int PASSES, int CBS, bool ENC>
-static cudaError_t launch_t(const Params &p, int grid, cudaStream_t st) {
+static cudaError_t launch_t(const Params &p, int grid, cudaStream_t st, bool lat) {
     using G = Geo<CBS>;
     const int warps_needed = (p.cb_end - p.cb_begin + G::NG - 1) / G::NG;
-    // A decode of at most half a wave of resident warps runs one warp per CTA:
-    // consecutive CTAs go to different SMs, so its heaviest codeblocks (the
-    // coarse subbands, neighbours in raster order) do not share an SM's
-    // instruction cache and shared-memory pipes (a 2048x2048 decode: 0.375 ->
-    // 0.358 ms).  Fuller decodes keep 4-warp CTAs, which measured faster there.
-    if (!ENC && grid <= 0 && 2LL * warps_needed <= (long long)resident_warps(false, -1))
-        return launch_w<PASSES, CBS, ENC, 1>(p, grid, warps_needed, st);
-    return launch_w<PASSES, CBS, ENC, kWarps>(p, grid, warps_needed, st);
+    const long long resident = resident_warps(ENC, -1);
+    if constexpr (ENC) {
+        // Encodes of at most two waves end with the serial chains of their
+        // heaviest codeblocks: the latency form of the symbol loop (a 2048x2048
+        // encode: 0.180 -> 0.167 ms).  Longer encodes are issue-bound and keep
+        // the form with fewer instructions.
+        if (lat && grid <= 0 && warps_needed <= 2 * resident)
+            return launch_w<PASSES, CBS, ENC, kWarps, true>(p, grid, warps_needed, st);
+        return launch_w<PASSES, CBS, ENC, kWarps, false>(p, grid, warps_needed, st);
+    } else {
+        // A decode of at most half a wave of resident warps runs one warp per
+        // CTA (consecutive CTAs go to different SMs, so its heaviest codeblocks,
+        // the coarse subbands, neighbours in raster order, do not share an SM's
+        // instruction cache and shared-memory pipes; a 2048x2048 decode: 0.375
+        // -> 0.358 ms) and the latency form of the step.  Fuller decodes keep
+        // 4-warp CTAs and the form with fewer instructions, which measured
+        // faster there.
+        if (lat && grid <= 0 && 2LL * warps_needed <= resident)
+            return launch_w<PASSES, CBS, ENC, 1, true>(p, grid, warps_needed, st);
+        return launch_w<PASSES, CBS, ENC, kWarps, false>(p, grid, warps_needed, st);
+    }
 }
 
-cudaError_t launch_code(bool enc, int passes, int cbs, const Params &p, int grid, cudaStream_t st) {
+cudaError_t launch_code(bool enc, int passes, int cbs, const Params &p, int grid, cudaStream_t st, bool lat) {
     if (p.cb_end <= p.cb_begin) return cudaSuccess;
     if (enc) {
-        if (passes == 2) return cbs == 64 ? launch_t<2, 64, true>(p, grid, st) : launch_t<2, 32, true>(p, grid, st);
-        return cbs == 64 ? launch_t<3, 64, true>(p, grid, st) : launch_t<3, 32, true>(p, grid, st);
+        if (passes == 2)
+            return cbs == 64 ? launch_t<2, 64, true>(p, grid, st, lat) : launch_t<2, 32, true>(p, grid, st, lat);
+        return cbs == 64 ? launch_t<3, 64, true>(p, grid, st, lat) : launch_t<3, 32, true>(p, grid, st, lat);
     }
-    if (passes == 2) return cbs == 64 ? launch_t<2, 64, false>(p, grid, st) : launch_t<2, 32, false>(p, grid, st);
-    return cbs == 64 ? launch_t<3, 64, false>(p, grid, st) : launch_t<3, 32, false>(p, grid, st);
+    if (passes == 2)
+        return cbs == 64 ? launch_t<2, 64, false>(p, grid, st, lat) : launch_t<2, 32, false>(p, grid, st, lat);
+    return cbs == 64 ? launch_t<3, 64, false>(p, grid, st, lat) : launch_t<3, 32, false>(p, grid, st, lat);
 }
 
 }  // namespace bpc

@@ -31,8 +31,19 @@ inline bool aligned_to(const void *p, unsigned a) { return ((uintptr_t)p & (uint
 
 // Launch the encoder (enc) or decoder over p.ncb codeblocks.  grid <= 0 picks
 // one CTA per kWarps codeblocks; a positive grid runs persistent CTAs that
-// walk the codeblocks grid-stride.
-cudaError_t launch_code(bool enc, int passes, int cbs, const Params &p, int grid, cudaStream_t st);
+// walk the codeblocks grid-stride.  latency_forms lets a launch of a few waves
+// take the latency forms of the coder loops (and one-warp CTAs for a small
+// decode), which finish a launch alone on the GPU sooner but execute more
+// instructions; callers that run many launches at once pass false.
+cudaError_t launch_code(bool enc, int passes, int cbs, const Params &p, int grid, cudaStream_t st,
+                        bool latency_forms = true);
+
+// One plain (sched null) or work-ordered launch over codeblocks
+// [cb_begin, cb_end) (cb_end < 0: all) after the C ABI's argument checks
+// (bpc_api.cu); returns a BPC_* code.
+int code_device(bool enc, const int *in, int *out, int X, int Y, const int *d_lut, int lut_n, int passes, int levels,
+                int cb, int *d_status, int *d_counts, int grid, void *stream, int cb_begin = 0, int cb_end = -1,
+                int *sched = nullptr, bool latency_forms = true);
 
 // Work order for a whole-image launch of many warp waves (bpc_order.cu): with
 // scratch `sched` of sched_ints(ncb, cbs) ints, queue the kernels that sort

@@ -128,16 +128,11 @@ void launch(Server *s, Slot &sl) {
     sl.st = sl.st_by_prio[priority_level(r.X, r.Y, (int)sl.st_by_prio.size())];
     int rc = cudaMemsetAsync(sl.d_status, 0, sizeof(int), sl.st) == cudaSuccess ? BPC_OK : BPC_ERR_CUDA;
     int *sched = r.sched_off ? reinterpret_cast<int *>(s->base + sl.off + r.sched_off) : nullptr;
-    if (!rc && sched)
-        rc = r.dir == BPC_CODE ? bpc_encode_device_sched(r.in, out, r.X, r.Y, L.d, L.n, L.passes, L.levels, r.cb,
-                                                         sl.d_status, nullptr, sched, sl.st)
-                               : bpc_decode_device_sched(r.in, out, r.X, r.Y, L.d, L.n, L.passes, L.levels, r.cb,
-                                                         sl.d_status, nullptr, sched, sl.st);
-    else if (!rc)
-        rc = r.dir == BPC_CODE ? bpc_encode_device(r.in, out, r.X, r.Y, L.d, L.n, L.passes, L.levels, r.cb,
-                                                   sl.d_status, nullptr, 0, sl.st)
-                               : bpc_decode_device(r.in, out, r.X, r.Y, L.d, L.n, L.passes, L.levels, r.cb,
-                                                   sl.d_status, nullptr, 0, sl.st);
+    // several requests share the SMs at once: the forms with the fewest
+    // instructions, not the latency forms of a launch alone on the GPU
+    if (!rc)
+        rc = bpc::code_device(r.dir == BPC_CODE, r.in, out, r.X, r.Y, L.d, L.n, L.passes, L.levels, r.cb, sl.d_status,
+                              nullptr, 0, sl.st, 0, -1, sched, false);
     if (!rc && cudaMemcpyAsync(sl.h_status, sl.d_status, sizeof(int), cudaMemcpyDeviceToHost, sl.st) != cudaSuccess)
         rc = BPC_ERR_CUDA;
     if (!rc && cudaEventRecord(sl.ev, sl.st) != cudaSuccess) rc = BPC_ERR_CUDA;

@@ -109,7 +109,7 @@ struct Job {
     uint32_t *ring;
     int base;
     unsigned long long *stats;
-    int kind;  // 0 code, 1 statistics
+    int kind;  // 0 code, 1 statistics, 2 code with the latency form of the loops
 };
 Job *J = nullptr;
 
@@ -120,6 +120,12 @@ void lane_main() {
     uint32_t planes[28][4];
     uint8_t ev_key[ENC ? bpc::kEvKeys : 1];
     uint32_t ev_val[ENC ? bpc::kEvVals : 1];
+    if (J->kind == 2) {  // the latency form of the loops
+        bpc::Coder<PASSES, CBS, ENC, EmuWarp, true> cd(w, *J->p, J->ring, J->tab, J->sgtab, planes, ev_key, ev_val);
+        cd.run(J->base);
+        S->done[l] = true;
+        return;
+    }
     bpc::Coder<PASSES, CBS, ENC, EmuWarp> cd(w, *J->p, J->ring, J->tab, J->sgtab, planes, ev_key, ev_val);
     if constexpr (ENC) {
         if (J->kind == 1)
@@ -175,9 +181,10 @@ int run_all(const bpc::Params &p, const uint8_t *tab, const uint8_t *sgtab, unsi
 
 }  // namespace
 
-// enc = 1 encode (kind 0: slot stream, kind 1: LUT statistics into stats),
-// enc = 0 decode (of the slot stream, or of the compact container when
-// offsets is not null).  Returns the OR of the status bits, or -1 if the lanes of a
+// enc = 1 encode (kind 0: slot stream, kind 1: LUT statistics into stats,
+// kind 2: slot stream with the latency form of the loops), enc = 0 decode (of
+// the slot stream, or of the compact container when offsets is not null; kind
+// 2: with the latency form).  Returns the OR of the status bits, or -1 if the lanes of a
 // warp ever met different collectives.
 extern "C" int emu_code(int enc, int kind, int passes, int cbs, const int32_t *in, int32_t *out, int X, int Y,
                         const int32_t *lut, int lut_n, int levels, unsigned long long *stats,
@@ -223,9 +230,9 @@ extern "C" int emu_code(int enc, int kind, int passes, int cbs, const int32_t *i
             rc = cbs == 64 ? run_all<3, 64, true>(p, t, g, stats, kind) : run_all<3, 32, true>(p, t, g, stats, kind);
     } else {
         if (passes == 2)
-            rc = cbs == 64 ? run_all<2, 64, false>(p, t, g, stats, 0) : run_all<2, 32, false>(p, t, g, stats, 0);
+            rc = cbs == 64 ? run_all<2, 64, false>(p, t, g, stats, kind) : run_all<2, 32, false>(p, t, g, stats, kind);
         else
-            rc = cbs == 64 ? run_all<3, 64, false>(p, t, g, stats, 0) : run_all<3, 32, false>(p, t, g, stats, 0);
+            rc = cbs == 64 ? run_all<3, 64, false>(p, t, g, stats, kind) : run_all<3, 32, false>(p, t, g, stats, kind);
     }
     S = nullptr;
     return rc ? rc : status;

@@ -39,15 +39,18 @@ def run(emu, enc, img_or_stream, shape, lut, passes, levels, cb, kind=0, stats=N
 
 
 def roundtrip(emu, oracle_mod, img, passes, levels, cb):
+    """Both forms of the coder loops (kind 0 and the latency form, kind 2)
+    against the oracle: streams, decodes, status bits."""
     lut = oracle_mod.load_luts(lut_folder(passes), passes, levels)
     want, wst = oracle_mod.encode(img, lut, passes, levels, cb, with_status=True)
-    got, st = run(emu, 1, img, img.shape, lut, passes, levels, cb)
-    np.testing.assert_array_equal(got, want)
-    assert st == int(np.bitwise_or.reduce(wst))
-    dec, dst = run(emu, 0, got, img.shape, lut, passes, levels, cb)
     wdec, wdst = oracle_mod.decode(want, img.shape, lut, passes, levels, cb, with_status=True)
-    np.testing.assert_array_equal(dec.reshape(img.shape), wdec)
-    assert dst == int(np.bitwise_or.reduce(wdst))
+    for kind in (0, 2):
+        got, st = run(emu, 1, img, img.shape, lut, passes, levels, cb, kind=kind)
+        np.testing.assert_array_equal(got, want)
+        assert st == int(np.bitwise_or.reduce(wst))
+        dec, dst = run(emu, 0, got, img.shape, lut, passes, levels, cb, kind=kind)
+        np.testing.assert_array_equal(dec.reshape(img.shape), wdec)
+        assert dst == int(np.bitwise_or.reduce(wdst))
     return st
 
 
