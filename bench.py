@@ -21,6 +21,7 @@ from __future__ import annotations
 import argparse
 import json
 import os
+import re
 import subprocess
 import sys
 import threading
@@ -101,7 +102,8 @@ def ncu_import(path, workload):
         if len(r) != len(names) or "k_bpc" not in r[col["Kernel Name"]] or "batch" in r[col["Kernel Name"]]:
             continue
         kname = r[col["Kernel Name"]]
-        kind = "encoder" if ("1>" in kname or "true>" in kname) else "decoder"
+        m = re.search(r"k_bpc<\s*\d+,\s*\d+,\s*(\w+)", kname)  # <passes, cb, encoder, ...>
+        kind = "encoder" if m and m.group(1) in ("1", "true") else "decoder"
         a = acc.setdefault(kind, [0, 0.0, 0.0, 0.0, 0.0])
         a[0] += 1
         a[1] += val(r, "gpu__time_duration.sum")

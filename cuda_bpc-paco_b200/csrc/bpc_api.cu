@@ -191,7 +191,7 @@ int code_device(bool enc, const int *in, int *out, int X, int Y, const int *d_lu
         p.cb_end = cb_end;
     }
     if (sched && grid <= 0) {
-        const cudaError_t e = plan_order(enc, cb, p, sched, (cudaStream_t)stream, &p.order);
+        const cudaError_t e = plan_order(enc, cb, p, sched, (cudaStream_t)stream, latency_forms);
         if (e != cudaSuccess) {
             std::fprintf(stderr, "bpc: work-order launch failed: %s\n", cudaGetErrorString(e));
             return BPC_ERR_CUDA;

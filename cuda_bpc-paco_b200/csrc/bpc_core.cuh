@@ -87,6 +87,12 @@ struct Params {
     // work order of a whole-image launch: warp slot k codes the codeblocks
     // starting at order[k] (null = raster order)
     const int *order = nullptr;
+    // isolated decode of a work-ordered image (launch_code): heavy = 1 codes
+    // the units order[0, heavy_n), one per warp slot; heavy = 2 codes the rest,
+    // one unit per warp slot first and then units taken from the queue counter
+    // *ctr (zeroed by the planner).  heavy = 0: the plain grid-stride walk.
+    int heavy = 0, heavy_n = 0;
+    int *ctr = nullptr;
 };
 
 // LUT offsets the reference kernel uses (Initialize_LUT_pointers :228-250 with

@@ -52,6 +52,10 @@ struct GpuWarp {
 template <int PASSES, int CBS, bool ENC, int WARPS = kWarps, bool LAT = false>
 __global__ void __launch_bounds__(WARPS * 32, (ENC ? kMinCtasEnc : kMinCtasDec) * kWarps / WARPS) k_bpc(Params p) {
     using G = Geo<CBS>;
+    const int heavy = ENC ? 0 : p.heavy;
+    // heavy launch of an isolated decode: the bulk launch (its programmatic
+    // dependent) may start as soon as every heavy CTA has reached this point
+    if (heavy == 1) asm volatile("griddepcontrol.launch_dependents;");
     extern __shared__ __align__(16) unsigned char smem[];
     uint8_t *tab = smem;
     int bad = 0;
@@ -75,11 +79,34 @@ __global__ void __launch_bounds__(WARPS * 32, (ENC ? kMinCtasEnc : kMinCtasDec) 
     uint32_t planes[28][4];  // per-thread bitplanes (local memory, L1-resident)
     uint8_t ev_key[ENC ? kEvKeys : 1];
     uint32_t ev_val[ENC ? kEvVals : 1];
-    const int stride = (int)gridDim.x * WARPS * G::NG;
-    for (int base = p.cb_begin + ((int)blockIdx.x * WARPS + warp) * G::NG; base < p.cb_end; base += stride) {
-        Coder<PASSES, CBS, ENC, GpuWarp, LAT> cd(w, p, ring, tab, sgtab, planes, ev_key, ev_val);
-        cd.run(p.order ? p.order[base / G::NG] : base);
+    // Walk: heavy 0, codeblocks cb_begin + slot*NG, grid-stride; heavy 1, the
+    // order's unit `slot` if slot < heavy_n; heavy 2, the order's unit
+    // heavy_n + slot, then the units past every warp slot's first one, each
+    // taken by the first warp to come back for work.
+    const int slot = (int)blockIdx.x * WARPS + warp, nslots = (int)gridDim.x * WARPS;
+    const int units = (p.ncb + G::NG - 1) / G::NG;
+    int pos = heavy == 1 ? (slot < p.heavy_n ? slot : p.heavy_n)
+                         : (heavy == 2 ? p.heavy_n + slot : p.cb_begin + slot * G::NG);
+    const int lim = heavy == 1 ? p.heavy_n : (heavy == 2 ? units : p.cb_end);
+    while (pos < lim) {
+        {
+            Coder<PASSES, CBS, ENC, GpuWarp, LAT> cd(w, p, ring, tab, sgtab, planes, ev_key, ev_val);
+            cd.run(heavy ? p.order[pos] : (p.order ? p.order[pos / G::NG] : pos));
+        }
+        if (heavy == 1) {
+            pos = lim;
+        } else if (heavy == 2) {
+            int nx = 0;
+            if ((threadIdx.x & 31u) == 0u) nx = atomicAdd(p.ctr, 1);
+            pos = p.heavy_n + nslots + __shfl_sync(0xffffffffu, nx, 0);
+        } else {
+            pos += nslots * G::NG;
+        }
     }
+    // bulk launch of an isolated decode: it completes only after the heavy
+    // launch, its programmatic prerequisite, has completed and its stores are
+    // visible, so whatever follows in the stream sees both
+    if (heavy == 2) asm volatile("griddepcontrol.wait;" ::: "memory");
 }
 
 // LUT training counts: the encoder's pass masks without its arithmetic coder
@@ -136,6 +163,61 @@ static cudaError_t launch_w(const Params &p, int grid, int warps_needed, cudaStr
     return cudaGetLastError();
 }
 
+// Isolated decode of a work-ordered image of one or two waves (p.order and
+// p.ctr from plan_order).  Its heaviest kIsoCtas x kWarps codeblocks run
+// first, in CTAs that take their SM's whole shared memory, so no other CTA
+// shares their SMs and each of their warps has a sub-partition to itself
+// (latency form of the step).  The rest of the image is a programmatic
+// dependent launch: it starts once every heavy CTA is resident, fills the other
+// SMs, one codeblock per warp slot, and the codeblocks beyond its warp slots go
+// to whichever warps finish first.  In a one-wave decode the heaviest
+// codeblocks' chains otherwise run beside 27 other warps and set the launch
+// time (4096x4096, 3-pass: 0.62 -> 0.55 ms).
+template <int PASSES, int CBS>
+static cudaError_t launch_iso(const Params &p, cudaStream_t st) {
+    using G = Geo<CBS>;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    const int optin = shared_optin(dev), sms = sm_count(dev);
+    if (optin <= 0 || sms <= kIsoCtas) return cudaErrorInvalidValue;
+    const int units = (p.ncb + G::NG - 1) / G::NG;
+    Params ph = p;
+    ph.heavy = 1;
+    ph.heavy_n = kIsoCtas * kWarps;
+    e = cudaFuncSetAttribute(k_bpc<PASSES, CBS, false, kWarps, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             optin);
+    if (e != cudaSuccess) return e;
+    k_bpc<PASSES, CBS, false, kWarps, true><<<kIsoCtas, kWarps * 32, (size_t)optin, st>>>(ph);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    Params pb = ph;
+    pb.heavy = 2;
+    const size_t sm = smem_bytes<PASSES, CBS, false, kWarps>(pb);
+    e = cudaFuncSetAttribute(k_bpc<PASSES, CBS, false, kWarps, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)sm);
+    if (e != cudaSuccess) return e;
+    int per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bpc<PASSES, CBS, false, kWarps, false>, kWarps * 32,
+                                                      sm);
+    if (e != cudaSuccess) return e;
+    const int full = (units - ph.heavy_n + kWarps - 1) / kWarps;
+    int grid = (sms - kIsoCtas) * (per_sm > 0 ? per_sm : 1);
+    if (grid > full) grid = full;
+    if (grid < 1) grid = 1;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)grid);
+    cfg.blockDim = dim3(kWarps * 32);
+    cfg.dynamicSmemBytes = sm;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, k_bpc<PASSES, CBS, false, kWarps, false>, pb);
+}
+
 template <int PASSES, int CBS, bool ENC>
 static cudaError_t launch_t(const Params &p, int grid, cudaStream_t st, bool lat) {
     using G = Geo<CBS>;
@@ -156,7 +238,11 @@ static cudaError_t launch_t(const Params &p, int grid, cudaStream_t st, bool lat
         // instruction cache and shared-memory pipes; a 2048x2048 decode: 0.375
         // -> 0.358 ms) and the latency form of the step.  Fuller decodes keep
         // 4-warp CTAs and the form with fewer instructions, which measured
-        // faster there.
+        // faster there.  A work-ordered whole image the planner marked for
+        // isolation (p.ctr set) runs its heaviest codeblocks on SMs of their own.
+        if constexpr (CBS == 64) {
+            if (lat && grid <= 0 && p.order && p.ctr) return launch_iso<PASSES, CBS>(p, st);
+        }
         if (lat && grid <= 0 && 2LL * warps_needed <= resident)
             return launch_w<PASSES, CBS, ENC, 1, true>(p, grid, warps_needed, st);
         return launch_w<PASSES, CBS, ENC, kWarps, false>(p, grid, warps_needed, st);

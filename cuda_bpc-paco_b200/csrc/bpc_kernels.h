@@ -45,16 +45,25 @@ int code_device(bool enc, const int *in, int *out, int X, int Y, const int *d_lu
                 int cb, int *d_status, int *d_counts, int grid, void *stream, int cb_begin = 0, int cb_end = -1,
                 int *sched = nullptr, bool latency_forms = true);
 
-// Work order for a whole-image launch of many warp waves (bpc_order.cu): with
-// scratch `sched` of sched_ints(ncb, cbs) ints, queue the kernels that sort
-// the image's work units by expected cost and set *order to the order to put
-// in Params; *order stays null (raster order) for images of at most two waves.
+// Work order for a whole-image launch (bpc_order.cu): with scratch `sched` of
+// sched_ints(ncb, cbs) ints, queue the kernels that sort the image's work
+// units by expected cost, heaviest first, and set p.order.  Images of more than
+// two waves are sorted for a balanced last wave; decodes of 64x64 codeblocks
+// between half a wave and two waves are sorted for an isolated launch
+// (launch_code) when `isolate` allows it, which also sets p.ctr to the bulk
+// launch's queue counter in the scratch.  Other images keep raster order
+// (p.order and p.ctr stay null).
 long long sched_ints(int ncb, int cbs);
+// SMs of device `dev`, and its opt-in shared memory per block (cached)
+int sm_count(int dev);
+int shared_optin(int dev);
 // warps of the plain coder resident at once on device `dev` (-1: current)
 int resident_warps(bool enc, int dev);
 // more than two waves on device `dev` (-1: the current device)
 bool order_pays(bool enc, int ncb, int cbs, int dev = -1);
-cudaError_t plan_order(bool enc, int cbs, const Params &p, int *sched, cudaStream_t st, const int **order);
+cudaError_t plan_order(bool enc, int cbs, Params &p, int *sched, cudaStream_t st, bool isolate);
+// heavy CTAs of an isolated decode (kWarps codeblocks each)
+constexpr int kIsoCtas = 6;
 
 // LUT training: add, per LUT entry, [2k] symbols coded and [2k+1] symbols
 // equal to 1 over p.ncb codeblocks of p.in (planes 0..14) to stats.

@@ -1,4 +1,5 @@
-// bpc_order.cu -- work order for images of several warp waves.
+// bpc_order.cu -- work order for images of several warp waves, and for the
+// isolated decode of images of one or two waves.
 //
 // A CTA of the coder keeps its slot on the SM until its slowest warp is done,
 // and the last wave of a launch runs on a partly idle GPU.  The time a warp
@@ -18,6 +19,10 @@
 //            from one read of the coefficients.
 // One CTA then counting-sorts the units by cost, descending (warp-aggregated
 // shared-memory atomics; units of equal cost in any order).
+//
+// An isolated decode (launch_code) takes the first units of the order for its
+// heavy launch and hands the rest out from a queue counter that follows the
+// order and the keys in the scratch; the sorting CTA zeroes it.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -32,11 +37,14 @@ namespace {
 constexpr int kBuckets = 1024;  // = threads of the sorting CTA
 // decoder cost per plane in codeword-equivalents: a lockstep pass over a plane
 // costs about as much as decoding 128 codewords (fit of per-codeblock decoder
-// cycles on a B200 to words + planes)
-constexpr uint32_t kPlaneWords = 128;
+// cycles on a B200 to words + planes).  For picking the few heaviest
+// codeblocks of an isolated decode the planes weigh double: the chains that
+// end last are those of the most planes (a 4096x4096 decode with 256: 0.560
+// ms; with 128: 0.597 ms; with 64: 0.601 ms).
+constexpr uint32_t kPlaneWords = 128, kPlaneWordsIso = 256;
 
 template <int CBS>
-__global__ void k_cost_dec(const int32_t *in, int ncb, uint32_t *key) {
+__global__ void k_cost_dec(const int32_t *in, int ncb, uint32_t plane_words, uint32_t *key) {
     using G = Geo<CBS>;
     const int units = (ncb + G::NG - 1) / G::NG;
     for (int u = (int)(blockIdx.x * blockDim.x + threadIdx.x); u < units; u += (int)(gridDim.x * blockDim.x)) {
@@ -55,7 +63,7 @@ __global__ void k_cost_dec(const int32_t *in, int ncb, uint32_t *key) {
             }
             const int m = __ldg(slot);  // MSB word: planes decoded
             const uint32_t planes = m == 32 ? 33u : (m >= 0 && m <= 27 ? (uint32_t)m + 1u : 0u);
-            cost += (uint32_t)lo + kPlaneWords * planes;
+            cost += (uint32_t)lo + plane_words * planes;
         }
         key[u] = cost;
     }
@@ -91,10 +99,12 @@ __device__ __forceinline__ int cost_bin(uint32_t cost, int shift) {
     return kBuckets - 1 - (int)(b > (uint32_t)(kBuckets - 1) ? (uint32_t)(kBuckets - 1) : b);
 }
 
-__global__ void __launch_bounds__(kBuckets) k_order(const uint32_t *key, int units, int shift, int ng, int *order) {
+__global__ void __launch_bounds__(kBuckets) k_order(const uint32_t *key, int units, int shift, int ng, int *order,
+                                                    int *ctr) {
     __shared__ uint32_t next[kBuckets];
     __shared__ uint32_t wsum[kBuckets / 32];
     const int tid = (int)threadIdx.x, lane = tid & 31;
+    if (tid == 0 && ctr) *ctr = 0;  // the isolated decode's queue counter
     next[tid] = 0;
     __syncthreads();
     // whole warps step through the units together (full-mask warp calls)
@@ -140,38 +150,64 @@ __global__ void __launch_bounds__(kBuckets) k_order(const uint32_t *key, int uni
 
 }  // namespace
 
-// warps resident at once on device `dev` (-1: the current device; SM count
-// cached per device; callers may be on any host thread)
-int resident_warps(bool enc, int dev) {
-    static std::atomic<int> sms[64];
-    if (dev < 0 && cudaGetDevice(&dev) != cudaSuccess) return 1 << 30;
-    if (dev < 0 || dev >= 64) return 1 << 30;
-    int n = sms[dev].load(std::memory_order_relaxed);
+namespace {
+// a device attribute, cached per device (callers may be on any host thread);
+// 0 if it cannot be read
+int cached_attr(cudaDeviceAttr a, std::atomic<int> *cache, int dev) {
+    if (dev < 0 || dev >= 64) return 0;
+    int n = cache[dev].load(std::memory_order_relaxed);
     if (!n) {
-        if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) return 1 << 30;
-        sms[dev].store(n, std::memory_order_relaxed);
+        if (cudaDeviceGetAttribute(&n, a, dev) != cudaSuccess || n <= 0) return 0;
+        cache[dev].store(n, std::memory_order_relaxed);
     }
+    return n;
+}
+}  // namespace
+
+int sm_count(int dev) {
+    static std::atomic<int> cache[64];
+    return cached_attr(cudaDevAttrMultiProcessorCount, cache, dev);
+}
+
+int shared_optin(int dev) {
+    static std::atomic<int> cache[64];
+    return cached_attr(cudaDevAttrMaxSharedMemoryPerBlockOptin, cache, dev);
+}
+
+// warps resident at once on device `dev` (-1: the current device)
+int resident_warps(bool enc, int dev) {
+    if (dev < 0 && cudaGetDevice(&dev) != cudaSuccess) return 1 << 30;
+    const int n = sm_count(dev);
+    if (n <= 0) return 1 << 30;
     return n * kWarps * (enc ? kMinCtasEnc : kMinCtasDec);
 }
 
 namespace {
 
 template <int CBS>
-cudaError_t plan_t(bool enc, const Params &p, int *sched, cudaStream_t st, const int **order) {
+cudaError_t plan_t(bool enc, Params &p, int *sched, cudaStream_t st, bool iso) {
     using G = Geo<CBS>;
     const int units = (p.ncb + G::NG - 1) / G::NG;
     uint32_t *key = reinterpret_cast<uint32_t *>(sched + units);
+    const uint32_t plane_words = iso ? kPlaneWordsIso : kPlaneWords;
     if (enc) {  // one warp per unit, grid-stride
         const int grid = (units + 7) / 8 < 4096 ? (units + 7) / 8 : 4096;
         k_cost_enc<CBS><<<grid, 256, 0, st>>>(p.in, p.X, p.ncbx, p.ncb, key);
     } else {  // one thread per unit, grid-stride
         const int grid = (units + 255) / 256 < 1024 ? (units + 255) / 256 : 1024;
-        k_cost_dec<CBS><<<grid, 256, 0, st>>>(p.in, p.ncb, key);
+        k_cost_dec<CBS><<<grid, 256, 0, st>>>(p.in, p.ncb, plane_words, key);
     }
-    // decoder costs reach NG * (CAP + 33 * kPlaneWords): 8320 (64x64), 12544 (32x32)
-    const int shift = enc ? 0 : (CBS == 64 ? 3 : 4);
-    k_order<<<1, kBuckets, 0, st>>>(key, units, shift, G::NG, sched);
-    *order = sched;
+    // bins of 2^shift cost units: decoder costs reach NG * (CAP + 33 * plane
+    // words), encoder costs 2 * 33
+    int shift = 0;
+    if (!enc) {
+        const long long mx = (long long)G::NG * ((long long)G::CAP + 33LL * plane_words);
+        while ((mx >> shift) > kBuckets - 1) shift++;
+    }
+    int *ctr = iso ? sched + 2 * units : nullptr;
+    k_order<<<1, kBuckets, 0, st>>>(key, units, shift, G::NG, sched, ctr);
+    p.order = sched;
+    p.ctr = ctr;
     return cudaGetLastError();
 }
 
@@ -179,21 +215,29 @@ cudaError_t plan_t(bool enc, const Params &p, int *sched, cudaStream_t st, const
 
 long long sched_ints(int ncb, int cbs) {
     const int ng = cbs == 64 ? 1 : 2;
-    return 2LL * ((ncb + ng - 1) / ng);
+    // order and cost keys, one int each per unit, then the queue counter
+    return 2LL * ((ncb + ng - 1) / ng) + 4;
 }
 
 bool order_pays(bool enc, int ncb, int cbs, int dev) {
     const int ng = cbs == 64 ? 1 : 2;
-    // an image within two waves gains nothing: every unit starts at once or
-    // in the second wave anyway, and the planning kernels cost more
+    // an image within two waves gains nothing from a balanced last wave: every
+    // unit starts at once or in the second wave anyway
     return (long long)((ncb + ng - 1) / ng) >= 2LL * resident_warps(enc, dev);
 }
 
-cudaError_t plan_order(bool enc, int cbs, const Params &p, int *sched, cudaStream_t st, const int **order) {
-    *order = nullptr;
-    if (!sched || p.offsets || p.cb_begin != 0 || p.cb_end != p.ncb || !order_pays(enc, p.ncb, cbs))
-        return cudaSuccess;
-    return cbs == 64 ? plan_t<64>(enc, p, sched, st, order) : plan_t<32>(enc, p, sched, st, order);
+cudaError_t plan_order(bool enc, int cbs, Params &p, int *sched, cudaStream_t st, bool isolate) {
+    p.order = nullptr;
+    p.ctr = nullptr;
+    if (!sched || p.offsets || p.cb_begin != 0 || p.cb_end != p.ncb) return cudaSuccess;
+    if (order_pays(enc, p.ncb, cbs))
+        return cbs == 64 ? plan_t<64>(enc, p, sched, st, false) : plan_t<32>(enc, p, sched, st, false);
+    // isolated decode: 64x64 codeblocks, more than half a wave (smaller decodes
+    // already spread one warp per CTA) and more than the heavy launch's share
+    const long long res = resident_warps(false, -1);
+    if (isolate && !enc && cbs == 64 && 2LL * p.ncb > res && p.ncb > 4 * kIsoCtas * kWarps)
+        return plan_t<64>(enc, p, sched, st, true);
+    return cudaSuccess;
 }
 
 }  // namespace bpc

@@ -131,12 +131,17 @@ int bpc_decode_device(const int *d_stream, int *d_coeffs, int X, int Y, const in
 /* The same calls with a work order: for images of more than two waves of
  * warps (above about 4,700 codeblocks for the encoder, 8,300 for the decoder
  * on a 148-SM B200) the call first sorts the codeblocks by expected work,
- * heaviest first (decoder: slot words in use; encoder: bitplanes coded, from
- * one read of the coefficients), so that the warps of a CTA finish together
- * and the last wave is short.  Outputs are identical to the calls above.
- * d_sched is the caller's device scratch of bpc_sched_ints(X, Y, cb_size)
- * ints (8 bytes per 64x64 codeblock), reusable once the call's stream has
- * passed it; still no allocation and no host sync. */
+ * heaviest first (decoder: slot words in use and bitplanes; encoder: bitplanes
+ * coded, from one read of the coefficients), so that the warps of a CTA finish
+ * together and the last wave is short.  A decode of 64x64 codeblocks between
+ * half a wave and two waves (about 2,100 to 8,300 codeblocks, e.g. 4096x4096)
+ * is sorted the same way and then isolated: its 24 heaviest codeblocks run on
+ * six SMs of their own, the rest on the other SMs as a programmatic dependent
+ * launch that starts once those are resident.  Outputs are identical to the
+ * calls above.  d_sched is the caller's device scratch of
+ * bpc_sched_ints(X, Y, cb_size) ints (8 bytes per 64x64 codeblock plus 16),
+ * reusable once the call's stream has passed it; still no allocation and no
+ * host sync. */
 long long bpc_sched_ints(int X, int Y, int cb_size);
 int bpc_encode_device_sched(const int *d_coeffs, int *d_stream, int X, int Y, const int *d_lut, int lut_n, int passes,
                             int levels, int cb_size, int *d_status, int *d_counts, int *d_sched, void *stream);

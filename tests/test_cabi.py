@@ -76,9 +76,10 @@ def test_host_band_plan(bpc, side, cb, setting):
 
 def test_sched_ints(bpc):
     L = bpc.lib()
-    assert L.bpc_sched_ints(4096, 4096, 64) == 2 * 4096
-    assert L.bpc_sched_ints(4096, 4096, 32) == 2 * 8192
-    assert L.bpc_sched_ints(96, 64, 32) == 2 * 3  # 6 codeblocks, 3 warp units
+    # order and cost key per warp unit, then 4 ints for the isolated decode's queue counter
+    assert L.bpc_sched_ints(4096, 4096, 64) == 2 * 4096 + 4
+    assert L.bpc_sched_ints(4096, 4096, 32) == 2 * 8192 + 4
+    assert L.bpc_sched_ints(96, 64, 32) == 2 * 3 + 4  # 6 codeblocks, 3 warp units
     for bad in ((100, 64, 64), (64, 64, 48), (0, 64, 64)):
         assert L.bpc_sched_ints(*bad) == bpc.ERR_ARG
 

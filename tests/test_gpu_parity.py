@@ -160,12 +160,15 @@ def test_host_pipeline_settings(bpc, cb):
 
 
 @pytest.mark.parametrize("side,levels,passes,cb", [(8192, 5, 3, 64), (6144, 6, 2, 64), (6144, 5, 3, 32),
-                                                     (2048, 5, 3, 64)])
+                                                     (2048, 5, 3, 64), (4096, 5, 3, 64), (3072, 5, 2, 64),
+                                                     (5120, 4, 3, 64)])
 def test_work_ordered_calls(bpc, side, levels, passes, cb):
     """The work-ordered entry points write the same stream and coefficients as
     the raster-order ones: images of many warp waves (sorted, 64x64 and 32x32
-    with codeblocks straddling subbands) and one within two waves (unsorted).
-    Outputs start from a sentinel, so a codeblock the order skipped shows."""
+    with codeblocks straddling subbands), one within half a wave (unsorted) and
+    decodes of one to two waves (4096, 3072, 5120: sorted and isolated, the 24
+    heaviest codeblocks on SMs of their own, the rest from a queue).  Outputs
+    start from a sentinel, so a codeblock the order skipped shows."""
     import torch
     lut = bpc.DeviceLut(lut_folder(passes), passes, levels)
     try:
