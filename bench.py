@@ -55,7 +55,7 @@ COUNTERS = os.path.join(ROOT, "profiles", "k_bpc_counters.txt")
 
 
 def load_counters():
-    """{(workload, kernel): {launches, time_us, dram_read, dram_write, warp_inst}}"""
+    """{(workload, direction): {calls, time_us, dram_read, dram_write, warp_inst}} per coder call"""
     out = {}
     try:
         with open(COUNTERS) as f:
@@ -63,7 +63,7 @@ def load_counters():
                 t = line.split()
                 if not t or t[0].startswith("#") or len(t) < 7:
                     continue
-                out[(t[0], t[1])] = {"launches": int(t[2]), "time_us": float(t[3]), "dram_read": float(t[4]),
+                out[(t[0], t[1])] = {"calls": int(t[2]), "time_us": float(t[3]), "dram_read": float(t[4]),
                                      "dram_write": float(t[5]), "warp_inst": float(t[6])}
     except OSError:
         pass
@@ -97,6 +97,8 @@ def ncu_import(path, workload):
             return per_s * val(r, "gpu__time_duration.sum") * 1e-6
         return 0.0
 
+    # per coder call: an isolated decode is a heavy launch of a few CTAs and
+    # the bulk launch after it, counted together as one call
     acc = {}
     for r in rows[hdr + 2:]:
         if len(r) != len(names) or "k_bpc" not in r[col["Kernel Name"]] or "batch" in r[col["Kernel Name"]]:
@@ -104,13 +106,15 @@ def ncu_import(path, workload):
         kname = r[col["Kernel Name"]]
         m = re.search(r"k_bpc<\s*\d+,\s*\d+,\s*(\w+)", kname)  # <passes, cb, encoder, ...>
         kind = "encoder" if m and m.group(1) in ("1", "true") else "decoder"
+        heavy = "launch__grid_size" in col and val(r, "launch__grid_size") <= 8
         a = acc.setdefault(kind, [0, 0.0, 0.0, 0.0, 0.0])
-        a[0] += 1
+        a[0] += 0 if heavy else 1
         a[1] += val(r, "gpu__time_duration.sum")
         a[2] += dram(r, "read")
         a[3] += dram(r, "write")
         a[4] += val(r, "smsp__inst_executed.sum")
     for kind, (n, t, rd, wr, ins) in sorted(acc.items()):
+        n = max(n, 1)
         print(f"{workload} {kind} {n} {t / n:.1f} {rd / n:.0f} {wr / n:.0f} {ins / n:.0f}")
 
 
@@ -123,11 +127,17 @@ def workload_name(c):
 def launches_per_call(X, Y, cb, enc, dev):
     """Kernels one work-ordered call launches: the coder, plus the cost and
     sort kernels when the image spans more than two waves of resident warps
-    (4 warps x 4 encoder / 7 decoder CTAs per SM)."""
+    (4 warps x 4 encoder / 7 decoder CTAs per SM); a decode of 64x64
+    codeblocks between half a wave and two waves is sorted too and isolated
+    (heavy launch + bulk launch)."""
     import torch
     units = (X // cb) * (Y // cb) // (1 if cb == 64 else 2)
     resident = torch.cuda.get_device_properties(dev).multi_processor_count * 4 * (4 if enc else 7)
-    return 3 if units >= 2 * resident else 1
+    if units >= 2 * resident:
+        return 3
+    if not enc and cb == 64 and 2 * units > resident and units > 4 * 6 * 4:
+        return 4
+    return 1
 
 
 def load_peaks():
@@ -780,16 +790,17 @@ def run_ours(args, c):
     dom = "decoder" if td1 >= te1 else "encoder"
     achieved = alg_bytes / dom_t / 1e9
     clocks = clk.summary()
-    # issue roofline: warp instructions of one launch of the dominant kernel
-    # (ncu capture of this workload) over what the SMs can issue in the
-    # launch's CUDA-event time at the clock sampled during the run
+    # issue roofline: warp instructions of one call of the dominant direction
+    # (ncu capture of this workload; an isolated decode's two launches
+    # together) over what the SMs can issue in the call's CUDA-event time at
+    # the clock sampled during the run
     cnt = load_counters().get((args.config, dom))
     sms = torch.cuda.get_device_properties(dev).multi_processor_count
     mhz = clocks.get("sm_mhz") or clocks.get("sm_max_mhz")
     issue = None
     if cnt and mhz:
         peak_inst = sms * 4 * mhz * 1e6  # one warp instruction per SM sub-partition per cycle
-        issue = {"warp_inst_per_launch": cnt["warp_inst"], "achieved_ginst_s": cnt["warp_inst"] / dom_t / 1e9,
+        issue = {"warp_inst_per_call": cnt["warp_inst"], "achieved_ginst_s": cnt["warp_inst"] / dom_t / 1e9,
                  "peak_ginst_s": peak_inst / 1e9, "frac": cnt["warp_inst"] / dom_t / peak_inst, "sm_mhz": mhz,
                  "sms": sms, "source": "profiles/k_bpc_counters.txt"}
     line = {
