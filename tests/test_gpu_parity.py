@@ -193,6 +193,53 @@ def test_work_ordered_calls(bpc, side, levels, passes, cb):
         lut.close()
 
 
+def test_isolated_decode_damaged_streams(bpc, oracle_mod):
+    """A 4096x4096 3-pass stream with damaged slots, LL codeblocks among them
+    (garbage codewords, MSB words 28-32, slots without the -1 fill), decodes
+    the same through the isolated work-ordered call, the plain call and the
+    oracle: coefficients and status bits.  The damage also changes the cost
+    order the isolated call plans from."""
+    import torch
+    side, levels, passes, cb = 4096, 5, 3, 64
+    lut = bpc.DeviceLut(lut_folder(passes), passes, levels)
+    try:
+        lut_np = oracle_mod.load_luts(lut_folder(passes), passes, levels)
+        d = bpc_synth.synthetic_coefficients_gpu(side, levels, 43, amp=60.0, nrect=100)
+        s_dev = torch.empty_like(d)
+        st = torch.zeros(3, dtype=torch.int32, device="cuda")
+        bpc.encode_device(d, s_dev, lut, cb, st[0:1])
+        slots = s_dev.cpu().numpy().reshape(-1, cb * cb).copy()
+        rng = np.random.default_rng(11)
+        ncb = slots.shape[0]
+        for k in (0, 1, 64, 65):  # LL codeblocks: garbage in their first used words
+            used = int(np.argmax(slots[k] == -1)) or cb * cb
+            slots[k, 1:used // 2] = rng.integers(0, 1 << 16, used // 2 - 1)
+        pick = rng.choice(np.arange(66, ncb), 48, replace=False)
+        for i, k in enumerate(pick):
+            if i % 4 == 0:
+                slots[k, 0] = 28 + (i // 4) % 4  # MSB words no encoder writes (28..31)
+            elif i % 4 == 1:
+                slots[k, 0] = 32  # all-zero claim over real codewords
+            elif i % 4 == 2:
+                slots[k, 1:] = rng.integers(0, 1 << 16, cb * cb - 1)  # no -1 fill
+            else:
+                slots[k, 1:9] = rng.integers(0, 1 << 16, 8)
+        damaged = slots.reshape(-1)
+        want, wst = oracle_mod.decode(damaged, (side, side), lut_np, passes, levels, cb, with_status=True)
+        s_in = torch.from_numpy(damaged).cuda()
+        plain = torch.full_like(d, 0x7F7F7F7F)
+        bpc.decode_device(s_in, plain, lut, cb, st[1:2])
+        iso = torch.full_like(d, 0x7F7F7F7F)
+        bpc.decode_device(s_in, iso, lut, cb, st[2:3], sched=bpc.sched_buffer(side, side, cb))
+        np.testing.assert_array_equal(plain.cpu().numpy(), want)
+        np.testing.assert_array_equal(iso.cpu().numpy(), want)
+        w = int(np.bitwise_or.reduce(wst))
+        assert w & bpc.ST_BAD_STREAM
+        assert st[1].item() == w and st[2].item() == w
+    finally:
+        lut.close()
+
+
 def test_drop_in_flow(bpc, oracle_mod, sample_subset):
     """main_example.cu:498-532: load_LUTs, CUDA_BPC(CODE), load_LUTs again
     (CUDA_BPC frees it), CUDA_BPC(DECODE), compare."""
