@@ -46,6 +46,9 @@ CONFIGS = {
     "cfg5": dict(side=16384, levels=5, passes=3, cb=64, amp=80.0, nrect=400, gpu_input=True),
     # cfg5's second input: i.i.d. Laplacian coefficients, every codeblock coding 16 planes
     "cfg5l": dict(side=16384, levels=5, passes=3, cb=64, laplacian=True, gpu_input=True),
+    # cfg5's generator at 8192x8192 (4 warp waves, work-ordered like cfg5): the
+    # case its ncu counters are captured on, under a GiB on the device
+    "cfg5s": dict(side=8192, levels=5, passes=3, cb=64, amp=80.0, nrect=400, gpu_input=True),
 }
 METRIC = "encode/decode Gcoeff/s (bit-exact)"
 # ncu counters of the coder kernels per workload, written by
@@ -70,7 +73,7 @@ def load_counters():
     return out
 
 
-def ncu_import(path, workload):
+def ncu_import(path, workload, units_scale=1.0):
     """Lines for COUNTERS from `ncu -i <rep> --page raw --csv` output: per
     coder kernel (encoder / decoder) the mean over its captured launches."""
     import csv
@@ -79,7 +82,8 @@ def ncu_import(path, workload):
     names, units = rows[hdr], rows[hdr + 1]
     col = {n: i for i, n in enumerate(names)}
     scale = {"byte": 1, "Kbyte": 1e3, "Mbyte": 1e6, "Gbyte": 1e9, "KB": 1e3, "MB": 1e6, "GB": 1e9,
-             "nsecond": 1e-3, "usecond": 1.0, "msecond": 1e3, "inst": 1, "Kinst": 1e3, "Minst": 1e6,
+             "nsecond": 1e-3, "usecond": 1.0, "msecond": 1e3, "ns": 1e-3, "us": 1.0, "ms": 1e3,
+             "inst": 1, "Kinst": 1e3, "Minst": 1e6,
              "Ginst": 1e9, "": 1}
 
     def val(r, m):
@@ -115,7 +119,8 @@ def ncu_import(path, workload):
         a[4] += val(r, "smsp__inst_executed.sum")
     for kind, (n, t, rd, wr, ins) in sorted(acc.items()):
         n = max(n, 1)
-        print(f"{workload} {kind} {n} {t / n:.1f} {rd / n:.0f} {wr / n:.0f} {ins / n:.0f}")
+        f = units_scale / n  # per call, times the workload's units over the captured case's
+        print(f"{workload} {kind} {n} {t * f:.1f} {rd * f:.0f} {wr * f:.0f} {ins * f:.0f}")
 
 
 def workload_name(c):
@@ -974,9 +979,11 @@ def main():
     ap.add_argument("--no-tune", action="store_true", help="cfg3: keep the default batch schedule")
     ap.add_argument("--ncu-import", help="print counter lines for profiles/k_bpc_counters.txt from ncu raw csv")
     ap.add_argument("--workload", default="cfg2", help="--ncu-import: workload name of the capture")
+    ap.add_argument("--scale", type=float, default=1.0,
+                    help="--ncu-import: units of the workload over units of the captured case")
     args = ap.parse_args()
     if args.ncu_import:
-        ncu_import(args.ncu_import, args.workload)
+        ncu_import(args.ncu_import, args.workload, args.scale)
         return
     if args.config in ("dwt", "train") and args.impl == "ours":
         (run_dwt if args.config == "dwt" else run_train)(args)
