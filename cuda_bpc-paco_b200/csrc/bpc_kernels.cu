@@ -215,7 +215,15 @@ static cudaError_t launch_iso(const Params &p, cudaStream_t st) {
     at[0].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = at;
     cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, k_bpc<PASSES, CBS, false, kWarps, false>, pb);
+    e = cudaLaunchKernelEx(&cfg, k_bpc<PASSES, CBS, false, kWarps, false>, pb);
+    if (e == cudaErrorNotSupported) {
+        // no programmatic launch here: the bulk then runs after the heavy
+        // launch in plain stream order (its final wait returns at once)
+        (void)cudaGetLastError();
+        cfg.numAttrs = 0;
+        e = cudaLaunchKernelEx(&cfg, k_bpc<PASSES, CBS, false, kWarps, false>, pb);
+    }
+    return e;
 }
 
 template <int PASSES, int CBS, bool ENC>
