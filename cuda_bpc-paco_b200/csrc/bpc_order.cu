@@ -233,9 +233,13 @@ cudaError_t plan_order(bool enc, int cbs, Params &p, int *sched, cudaStream_t st
     if (order_pays(enc, p.ncb, cbs))
         return cbs == 64 ? plan_t<64>(enc, p, sched, st, false) : plan_t<32>(enc, p, sched, st, false);
     // isolated decode: 64x64 codeblocks, more than half a wave (smaller decodes
-    // already spread one warp per CTA) and more than the heavy launch's share
-    const long long res = resident_warps(false, -1);
-    if (isolate && !enc && cbs == 64 && 2LL * p.ncb > res && p.ncb > 4 * kIsoCtas * kWarps)
+    // already spread one warp per CTA), more than the heavy launch's share, and
+    // a device with SMs to spare for it
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return cudaSuccess;
+    const long long res = resident_warps(false, dev);
+    if (isolate && !enc && cbs == 64 && 2LL * p.ncb > res && p.ncb > 4 * kIsoCtas * kWarps &&
+        sm_count(dev) > 4 * kIsoCtas && shared_optin(dev) > 0)
         return plan_t<64>(enc, p, sched, st, true);
     return cudaSuccess;
 }
