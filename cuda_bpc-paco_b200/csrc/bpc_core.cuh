@@ -476,8 +476,8 @@ struct Coder {
     BPC_FI void dec_ctx_step(int j, int c_rt, int b, bool act) {
         const int c = CC >= 0 ? CC : c_rt;
         const uint64_t S0 = s.S[0], S1 = s.S[1], Sc = c ? S1 : S0;
+        // the caller runs the step only if some lane has a candidate here
         const bool cand = act && (PK == PK_SPP ? !bith<H>(Sc, j) : bith<H>(c ? s.C[1] : s.C[0], j));
-        if (!w.any(cand)) return;
         const uint64_t Lm = c ? S0 : s.XL, Rm = c ? s.XR : S1;
         const uint32_t wl = win3h<H>(Lm, j), wm = win3h<H>(Sc, j), wr = win3h<H>(Rm, j);
         const uint32_t nbh = wl | ((wm & 5u) << 3) | (wr << 6);
@@ -549,14 +549,19 @@ struct Coder {
         }
     }
 
+    // u0 / u1: the rows of this half where some lane has a candidate in column
+    // 0 / 1.  A step's candidates change only at the step itself (a coefficient
+    // becomes significant, or leaves CP, when it is coded), so the pass's masks
+    // taken at its start pick the steps to run, with no vote per step.
     template <int PK, int H>
-    BPC_FI void dec_ctx_half(uint32_t u, int b, bool act) {
+    BPC_FI void dec_ctx_half(uint32_t u0, uint32_t u1, int b, bool act) {
+        uint32_t u = u0 | u1;
         while (u) {
             const int j = ctz32(u);
             u &= u - 1;
             ring_ensure<4>();  // one row: two steps of up to two AC calls
-            dec_ctx_step<PK, H, 0>(j, 0, b, act);
-            dec_ctx_step<PK, H, 1>(j, 1, b, act);
+            if ((u0 >> j) & 1u) dec_ctx_step<PK, H, 0>(j, 0, b, act);
+            if ((u1 >> j) & 1u) dec_ctx_step<PK, H, 1>(j, 1, b, act);
         }
     }
 
@@ -567,16 +572,15 @@ struct Coder {
         sign_base = off + p.a_sign + (g + b) * 4;
         const uint64_t c0 = act ? (PK == PK_SPP ? ~s.S[0] : s.C[0]) : 0ull;
         const uint64_t c1 = act ? (PK == PK_SPP ? ~s.S[1] : s.C[1]) : 0ull;
-        const uint64_t U = warp_or64(w, (c0 | c1) & G::ROWS);
-        dec_ctx_half<PK, 0>((uint32_t)U, b, act);
-        if (CBS == 64) dec_ctx_half<PK, 1>((uint32_t)(U >> 32), b, act);
+        const uint64_t U0 = warp_or64(w, c0 & G::ROWS), U1 = warp_or64(w, c1 & G::ROWS);
+        dec_ctx_half<PK, 0>((uint32_t)U0, (uint32_t)U1, b, act);
+        if (CBS == 64) dec_ctx_half<PK, 1>((uint32_t)(U0 >> 32), (uint32_t)(U1 >> 32), b, act);
     }
 
     // MRP_Decoder :608-629
     template <int H>
     BPC_FI void dec_mrp_step(int j, int c, int b, bool act, uint32_t P) {
         const bool cand = act && bith<H>(c ? s.R[1] : s.R[0], j);
-        if (!w.any(cand)) return;
         const uint32_t sym = ac_dec(cand, P);
         if (cand && sym && b <= 27) {
             const uint64_t bit = maskh<H>(1u, j);
@@ -584,22 +588,25 @@ struct Coder {
             B[1] |= c ? bit : 0ull;
         }
     }
+    // u0 / u1 as in dec_ctx_half (the refinement set is fixed during the pass)
     template <int H>
-    BPC_FI void dec_mrp_half(uint32_t u, int b, bool act, uint32_t P) {
+    BPC_FI void dec_mrp_half(uint32_t u0, uint32_t u1, int b, bool act, uint32_t P) {
+        uint32_t u = u0 | u1;
         while (u) {
             const int j = ctz32(u);
             u &= u - 1;
             ring_ensure<2>();  // one row: two steps of one AC call
-            dec_mrp_step<H>(j, 0, b, act, P);
-            dec_mrp_step<H>(j, 1, b, act, P);
+            if ((u0 >> j) & 1u) dec_mrp_step<H>(j, 0, b, act, P);
+            if ((u1 >> j) & 1u) dec_mrp_step<H>(j, 1, b, act, P);
         }
     }
 
     BPC_FI void dec_mrp_pass(int b, bool act) {
         const uint32_t P = act ? tab[g + b] : 0u;
-        const uint64_t U = warp_or64(w, act ? ((s.R[0] | s.R[1]) & G::ROWS) : 0ull);
-        dec_mrp_half<0>((uint32_t)U, b, act, P);
-        if (CBS == 64) dec_mrp_half<1>((uint32_t)(U >> 32), b, act, P);
+        const uint64_t U0 = warp_or64(w, act ? (s.R[0] & G::ROWS) : 0ull);
+        const uint64_t U1 = warp_or64(w, act ? (s.R[1] & G::ROWS) : 0ull);
+        dec_mrp_half<0>((uint32_t)U0, (uint32_t)U1, b, act, P);
+        if (CBS == 64) dec_mrp_half<1>((uint32_t)(U0 >> 32), (uint32_t)(U1 >> 32), b, act, P);
         if (act) {
             s.R[0] = s.S[0];
             s.R[1] = s.S[1];
