@@ -9,6 +9,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <mutex>
+
 #include "bpc_core.cuh"
 #include "bpc_kernels.h"
 
@@ -150,8 +152,18 @@ static size_t smem_bytes(const Params &p) {
     return (size_t)p.tab_n + (size_t)kSignTableBytes + (size_t)WARPS * 4u * (size_t)(ENC ? 512 : G::RING_WORDS);
 }
 
+// The shared memory a launch asks for grows with the LUT's length, and the
+// attribute that admits it belongs to the kernel, not to the launch: host
+// threads set it and launch under this lock, so no launch meets a smaller
+// setting another thread made in between.
+static std::mutex &attr_mu() {
+    static std::mutex m;
+    return m;
+}
+
 template <int PASSES, int CBS, bool ENC, int WARPS, bool LAT>
 static cudaError_t launch_w(const Params &p, int grid, int warps_needed, cudaStream_t st) {
+    std::lock_guard<std::mutex> lk(attr_mu());
     const size_t sm = smem_bytes<PASSES, CBS, ENC, WARPS>(p);
     cudaError_t e = cudaFuncSetAttribute(k_bpc<PASSES, CBS, ENC, WARPS, LAT>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
@@ -176,6 +188,7 @@ static cudaError_t launch_w(const Params &p, int grid, int warps_needed, cudaStr
 template <int PASSES, int CBS>
 static cudaError_t launch_iso(const Params &p, cudaStream_t st) {
     using G = Geo<CBS>;
+    std::lock_guard<std::mutex> lk(attr_mu());
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
