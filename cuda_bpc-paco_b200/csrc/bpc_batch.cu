@@ -756,9 +756,12 @@ int bpc_batch_tune(void *batch, const int *const *d_coeffs, int *d_compact, long
     // coarse-subbands-first queue
     if (const int rc0 = bpc_batch_set_tuning(batch, kWarps, kWarps, 0, 0, 0, 0)) return rc0;
     int bi = b->per_item, be = b->ctas_enc, bd = b->ctas_dec;
+    // the fastest of three runs after one that may capture the graph: the
+    // candidates differ by a few percent, about a run's spread, and the
+    // minimum is the least disturbed of the three
     auto timed = [&](bool enc, float &ms) -> int {
-        float acc = 0.f;
-        for (int r = 0; r < 3; r++) {
+        float best_run = 1e30f;
+        for (int r = 0; r < 4; r++) {
             CUDA_TRY(cudaEventRecord(e0, st));
             const int rc = enc ? bpc_batch_encode(batch, d_coeffs, d_compact, d_offsets, nullptr, stream)
                                : bpc_batch_decode(batch, d_compact, d_offsets, d_out, nullptr, stream);
@@ -767,9 +770,9 @@ int bpc_batch_tune(void *batch, const int *const *d_coeffs, int *d_compact, long
             CUDA_TRY(cudaEventSynchronize(e1));
             float t;
             CUDA_TRY(cudaEventElapsedTime(&t, e0, e1));
-            if (r) acc += t;  // the first run may capture the graph
+            if (r && t < best_run) best_run = t;  // the first run may capture the graph
         }
-        ms = acc / 2.f;
+        ms = best_run;
         return BPC_OK;
     };
     for (int it : items) {
