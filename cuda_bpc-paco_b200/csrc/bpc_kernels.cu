@@ -184,7 +184,7 @@ static cudaError_t launch_w(const Params &p, int grid, int warps_needed, cudaStr
 // SMs, one codeblock per warp slot, and the codeblocks beyond its warp slots go
 // to whichever warps finish first.  In a one-wave decode the heaviest
 // codeblocks' chains otherwise run beside 27 other warps and set the launch
-// time (4096x4096, 3-pass: 0.62 -> 0.55 ms).
+// time (4096x4096, 3-pass: 0.62 -> 0.54 ms).
 template <int PASSES, int CBS>
 static cudaError_t launch_iso(const Params &p, cudaStream_t st) {
     using G = Geo<CBS>;
