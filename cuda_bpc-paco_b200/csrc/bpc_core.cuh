@@ -328,11 +328,12 @@ BPC_FI uint64_t shfl_down64(W &w, uint64_t v) {
 
 // LAT selects the latency form of the per-lane loops, for launches whose time is
 // the serial chain of their heaviest codeblocks rather than the SMs' issue rate:
-// the encoder codes two positions per loop iteration (two independent
-// extractions and table reads ahead of the two sequential coder updates), the
-// decoder reads a step's sign context before its significance decision.  Both
-// execute more instructions per symbol; the bitstream is the same.
-template <int PASSES, int CBS, bool ENC, class W, bool LAT = false>
+// the encoder codes LAT + 1 positions per loop iteration (independent
+// extractions and table reads ahead of the sequential coder updates), the
+// decoder (any LAT > 0) reads a step's sign context before its significance
+// decision.  They execute more instructions per symbol; the bitstream is the
+// same.  LAT = 0 is the base form.
+template <int PASSES, int CBS, bool ENC, class W, int LAT = 0>
 struct Coder {
     using G = Geo<CBS>;
     static constexpr int NH = CBS / 32;  // 32-row halves per column
@@ -495,7 +496,7 @@ struct Coder {
             se = sgtab[sk];
             P2e = tab[sign_base + (int)(se & 3u)];
         };
-        if (LAT) sign_ctx();
+        if (LAT > 0) sign_ctx();
         bool coded = cand;
         if (PK == PK_SPP && PASSES == 3) {
             if (cand && nbh == 0) {  // SPP defers to CP (:450-452)
@@ -524,7 +525,7 @@ struct Coder {
         }
         if (!w.any(ns)) return;
         // sign call
-        if (!LAT) sign_ctx();
+        if (LAT == 0) sign_ctx();
         const uint32_t pred = se >> 2;
         const uint32_t P2 = ns ? P2e : 0u;
         const uint32_t neg = (ac_dec(ns, P2) ^ pred) & 1u;
@@ -884,6 +885,11 @@ struct Coder {
         }
     }
 
+    // significance context of position t from its four bit slices
+    static BPC_FI uint32_t ctx4(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, int t) {
+        return ((c0 >> t) & 1u) | (((c1 >> t) & 1u) << 1) | (((c2 >> t) & 1u) << 2) | (((c3 >> t) & 1u) << 3);
+    }
+
     template <int PK>
     BPC_FI void enc_pass_code(int b, bool act) {
         const int off = PK == PK_CP ? p.cp_off : 0;
@@ -907,7 +913,39 @@ struct Coder {
                 s1 = zip16(si[0][1], si[1][1], q);
                 gq = zip16(sg[0], sg[1], q);
             }
-            if constexpr (LAT) {  // two positions per iteration, the second predicated
+            if constexpr (LAT >= 2) {  // three positions per iteration, the later ones predicated
+                do {
+                    const int t = ctz32(kq);
+                    kq &= kq - 1;
+                    const bool two = kq != 0u;
+                    const int t2 = two ? ctz32(kq) : t;
+                    kq &= two ? kq - 1 : kq;
+                    const bool three = kq != 0u;
+                    const int t3 = three ? ctz32(kq) : t;
+                    kq &= three ? kq - 1 : kq;
+                    const int key = (32 * q + t) * 2, key2 = (32 * q + t2) * 2, key3 = (32 * q + t3) * 2;
+                    if (PK == PK_MRP) {
+                        enc_symbol_if(true, (yq >> t) & 1u, Pref, key);
+                        enc_symbol_if(two, (yq >> t2) & 1u, Pref, key2);
+                        enc_symbol_if(three, (yq >> t3) & 1u, Pref, key3);
+                    } else {
+                        const uint32_t ca = ctx4(c0, c1, c2, c3, t), cb2 = ctx4(c0, c1, c2, c3, t2);
+                        const uint32_t cc3 = ctx4(c0, c1, c2, c3, t3);
+                        const uint32_t sa = ((s0 >> t) & 1u) | (((s1 >> t) & 1u) << 1);
+                        const uint32_t sb = ((s0 >> t2) & 1u) | (((s1 >> t2) & 1u) << 1);
+                        const uint32_t sc = ((s0 >> t3) & 1u) | (((s1 >> t3) & 1u) << 1);
+                        const uint32_t Pa = tab[sig_b + (int)ca], P2a = tab[sign_b + (int)sa];
+                        const uint32_t Pb = tab[sig_b + (int)cb2], P2b = tab[sign_b + (int)sb];
+                        const uint32_t Pc = tab[sig_b + (int)cc3], P2c = tab[sign_b + (int)sc];
+                        enc_symbol_if(true, (yq >> t) & 1u, Pa, key);
+                        enc_symbol_if(((nq >> t) & 1u) != 0u, (gq >> t) & 1u, P2a, key + 1);
+                        enc_symbol_if(two, (yq >> t2) & 1u, Pb, key2);
+                        enc_symbol_if(two && ((nq >> t2) & 1u) != 0u, (gq >> t2) & 1u, P2b, key2 + 1);
+                        enc_symbol_if(three, (yq >> t3) & 1u, Pc, key3);
+                        enc_symbol_if(three && ((nq >> t3) & 1u) != 0u, (gq >> t3) & 1u, P2c, key3 + 1);
+                    }
+                } while (kq);
+            } else if constexpr (LAT == 1) {  // two positions per iteration, the second predicated
                 do {
                     const int t = ctz32(kq);
                     kq &= kq - 1;
@@ -919,10 +957,7 @@ struct Coder {
                         enc_symbol_if(true, (yq >> t) & 1u, Pref, key);
                         enc_symbol_if(two, (yq >> t2) & 1u, Pref, key2);
                     } else {
-                        const uint32_t ca = ((c0 >> t) & 1u) | (((c1 >> t) & 1u) << 1) | (((c2 >> t) & 1u) << 2) |
-                                            (((c3 >> t) & 1u) << 3);
-                        const uint32_t cb2 = ((c0 >> t2) & 1u) | (((c1 >> t2) & 1u) << 1) | (((c2 >> t2) & 1u) << 2) |
-                                             (((c3 >> t2) & 1u) << 3);
+                        const uint32_t ca = ctx4(c0, c1, c2, c3, t), cb2 = ctx4(c0, c1, c2, c3, t2);
                         const uint32_t sa = ((s0 >> t) & 1u) | (((s1 >> t) & 1u) << 1);
                         const uint32_t sb = ((s0 >> t2) & 1u) | (((s1 >> t2) & 1u) << 1);
                         const uint32_t Pa = tab[sig_b + (int)ca], P2a = tab[sign_b + (int)sa];
@@ -941,8 +976,7 @@ struct Coder {
                     if (PK == PK_MRP) {
                         enc_symbol_if(true, (yq >> t) & 1u, Pref, key);
                     } else {
-                        const uint32_t ctx = ((c0 >> t) & 1u) | (((c1 >> t) & 1u) << 1) |
-                                             (((c2 >> t) & 1u) << 2) | (((c3 >> t) & 1u) << 3);
+                        const uint32_t ctx = ctx4(c0, c1, c2, c3, t);
                         enc_symbol_if(true, (yq >> t) & 1u, tab[sig_b + (int)ctx], key);
                         // the sign call of a coefficient that became significant
                         const uint32_t sidx = ((s0 >> t) & 1u) | (((s1 >> t) & 1u) << 1);

@@ -51,7 +51,7 @@ struct GpuWarp {
 // WARPS codeblock warps per CTA: kWarps, or 1 for decodes of at most half a wave
 // (their heaviest codeblocks then land on different SMs, see launch_t); the
 // register budget stays that of kMinCtas x kWarps resident warps per SM
-template <int PASSES, int CBS, bool ENC, int WARPS = kWarps, bool LAT = false>
+template <int PASSES, int CBS, bool ENC, int WARPS = kWarps, int LAT = 0>
 __global__ void __launch_bounds__(WARPS * 32, (ENC ? kMinCtasEnc : kMinCtasDec) * kWarps / WARPS) k_bpc(Params p) {
     using G = Geo<CBS>;
     const int heavy = ENC ? 0 : p.heavy;
@@ -161,7 +161,7 @@ static std::mutex &attr_mu() {
     return m;
 }
 
-template <int PASSES, int CBS, bool ENC, int WARPS, bool LAT>
+template <int PASSES, int CBS, bool ENC, int WARPS, int LAT>
 static cudaError_t launch_w(const Params &p, int grid, int warps_needed, cudaStream_t st) {
     std::lock_guard<std::mutex> lk(attr_mu());
     const size_t sm = smem_bytes<PASSES, CBS, ENC, WARPS>(p);
@@ -198,20 +198,20 @@ static cudaError_t launch_iso(const Params &p, cudaStream_t st) {
     Params ph = p;
     ph.heavy = 1;
     ph.heavy_n = kIsoCtas * kWarps;
-    e = cudaFuncSetAttribute(k_bpc<PASSES, CBS, false, kWarps, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    e = cudaFuncSetAttribute(k_bpc<PASSES, CBS, false, kWarps, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              optin);
     if (e != cudaSuccess) return e;
-    k_bpc<PASSES, CBS, false, kWarps, true><<<kIsoCtas, kWarps * 32, (size_t)optin, st>>>(ph);
+    k_bpc<PASSES, CBS, false, kWarps, 1><<<kIsoCtas, kWarps * 32, (size_t)optin, st>>>(ph);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     Params pb = ph;
     pb.heavy = 2;
     const size_t sm = smem_bytes<PASSES, CBS, false, kWarps>(pb);
-    e = cudaFuncSetAttribute(k_bpc<PASSES, CBS, false, kWarps, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    e = cudaFuncSetAttribute(k_bpc<PASSES, CBS, false, kWarps, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)sm);
     if (e != cudaSuccess) return e;
     int per_sm = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bpc<PASSES, CBS, false, kWarps, false>, kWarps * 32,
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bpc<PASSES, CBS, false, kWarps, 0>, kWarps * 32,
                                                       sm);
     if (e != cudaSuccess) return e;
     const int full = (units - ph.heavy_n + kWarps - 1) / kWarps;
@@ -228,13 +228,13 @@ static cudaError_t launch_iso(const Params &p, cudaStream_t st) {
     at[0].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = at;
     cfg.numAttrs = 1;
-    e = cudaLaunchKernelEx(&cfg, k_bpc<PASSES, CBS, false, kWarps, false>, pb);
+    e = cudaLaunchKernelEx(&cfg, k_bpc<PASSES, CBS, false, kWarps, 0>, pb);
     if (e == cudaErrorNotSupported) {
         // no programmatic launch here: the bulk then runs after the heavy
         // launch in plain stream order (its final wait returns at once)
         (void)cudaGetLastError();
         cfg.numAttrs = 0;
-        e = cudaLaunchKernelEx(&cfg, k_bpc<PASSES, CBS, false, kWarps, false>, pb);
+        e = cudaLaunchKernelEx(&cfg, k_bpc<PASSES, CBS, false, kWarps, 0>, pb);
     }
     return e;
 }
@@ -246,12 +246,16 @@ static cudaError_t launch_t(const Params &p, int grid, cudaStream_t st, bool lat
     const long long resident = resident_warps(ENC, -1);
     if constexpr (ENC) {
         // Encodes of at most two waves end with the serial chains of their
-        // heaviest codeblocks: the latency form of the symbol loop (a 2048x2048
-        // encode: 0.180 -> 0.167 ms).  Longer encodes are issue-bound and keep
-        // the form with fewer instructions.
+        // heaviest codeblocks: the latency forms of the symbol loop, three
+        // positions per iteration within one wave (a 2048x2048 encode: 0.180
+        // -> 0.154 ms), two within two waves (4096x4096: 0.417 -> 0.412 ms;
+        // three there: 0.430).  Longer encodes are issue-bound and keep the
+        // form with fewer instructions.
+        if (lat && grid <= 0 && warps_needed <= resident)
+            return launch_w<PASSES, CBS, ENC, kWarps, 2>(p, grid, warps_needed, st);
         if (lat && grid <= 0 && warps_needed <= 2 * resident)
-            return launch_w<PASSES, CBS, ENC, kWarps, true>(p, grid, warps_needed, st);
-        return launch_w<PASSES, CBS, ENC, kWarps, false>(p, grid, warps_needed, st);
+            return launch_w<PASSES, CBS, ENC, kWarps, 1>(p, grid, warps_needed, st);
+        return launch_w<PASSES, CBS, ENC, kWarps, 0>(p, grid, warps_needed, st);
     } else {
         // A decode of at most half a wave of resident warps runs one warp per
         // CTA (consecutive CTAs go to different SMs, so its heaviest codeblocks,
@@ -265,8 +269,8 @@ static cudaError_t launch_t(const Params &p, int grid, cudaStream_t st, bool lat
             if (lat && grid <= 0 && p.order && p.ctr) return launch_iso<PASSES, CBS>(p, st);
         }
         if (lat && grid <= 0 && 2LL * warps_needed <= resident)
-            return launch_w<PASSES, CBS, ENC, 1, true>(p, grid, warps_needed, st);
-        return launch_w<PASSES, CBS, ENC, kWarps, false>(p, grid, warps_needed, st);
+            return launch_w<PASSES, CBS, ENC, 1, 1>(p, grid, warps_needed, st);
+        return launch_w<PASSES, CBS, ENC, kWarps, 0>(p, grid, warps_needed, st);
     }
 }
 

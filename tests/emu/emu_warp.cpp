@@ -109,7 +109,7 @@ struct Job {
     uint32_t *ring;
     int base;
     unsigned long long *stats;
-    int kind;  // 0 code, 1 statistics, 2 code with the latency form of the loops
+    int kind;  // 0 code, 1 statistics, 2 / 3 code with the latency forms of the loops (LAT 1 / 2)
 };
 Job *J = nullptr;
 
@@ -120,8 +120,14 @@ void lane_main() {
     uint32_t planes[28][4];
     uint8_t ev_key[ENC ? bpc::kEvKeys : 1];
     uint32_t ev_val[ENC ? bpc::kEvVals : 1];
-    if (J->kind == 2) {  // the latency form of the loops
-        bpc::Coder<PASSES, CBS, ENC, EmuWarp, true> cd(w, *J->p, J->ring, J->tab, J->sgtab, planes, ev_key, ev_val);
+    if (J->kind == 2) {  // the latency forms of the loops
+        bpc::Coder<PASSES, CBS, ENC, EmuWarp, 1> cd(w, *J->p, J->ring, J->tab, J->sgtab, planes, ev_key, ev_val);
+        cd.run(J->base);
+        S->done[l] = true;
+        return;
+    }
+    if (J->kind == 3) {
+        bpc::Coder<PASSES, CBS, ENC, EmuWarp, 2> cd(w, *J->p, J->ring, J->tab, J->sgtab, planes, ev_key, ev_val);
         cd.run(J->base);
         S->done[l] = true;
         return;
@@ -182,7 +188,7 @@ int run_all(const bpc::Params &p, const uint8_t *tab, const uint8_t *sgtab, unsi
 }  // namespace
 
 // enc = 1 encode (kind 0: slot stream, kind 1: LUT statistics into stats,
-// kind 2: slot stream with the latency form of the loops), enc = 0 decode (of
+// kind 2 / 3: slot stream with the latency forms of the loops), enc = 0 decode (of
 // the slot stream, or of the compact container when offsets is not null; kind
 // 2: with the latency form).  Returns the OR of the status bits, or -1 if the lanes of a
 // warp ever met different collectives.

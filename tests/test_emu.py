@@ -39,12 +39,13 @@ def run(emu, enc, img_or_stream, shape, lut, passes, levels, cb, kind=0, stats=N
 
 
 def roundtrip(emu, oracle_mod, img, passes, levels, cb):
-    """Both forms of the coder loops (kind 0 and the latency form, kind 2)
-    against the oracle: streams, decodes, status bits."""
+    """Every form of the coder loops (kind 0; the latency forms, kinds 2 and 3:
+    two and three encoder positions per iteration) against the oracle:
+    streams, decodes, status bits."""
     lut = oracle_mod.load_luts(lut_folder(passes), passes, levels)
     want, wst = oracle_mod.encode(img, lut, passes, levels, cb, with_status=True)
     wdec, wdst = oracle_mod.decode(want, img.shape, lut, passes, levels, cb, with_status=True)
-    for kind in (0, 2):
+    for kind in (0, 2, 3):
         got, st = run(emu, 1, img, img.shape, lut, passes, levels, cb, kind=kind)
         np.testing.assert_array_equal(got, want)
         assert st == int(np.bitwise_or.reduce(wst))
